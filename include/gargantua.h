@@ -1,0 +1,254 @@
+/*
+ * gargantua-b200: the per-frame compute of gargantua (particle sim,
+ * cloud-in-cell splat and resolve, null-geodesic march, probes, bake and
+ * walk, tone curve) as sm_100a kernels behind a plain C interface.
+ *
+ * The interface replaces the Metal passes a gargantua host encodes
+ * (Sources/Gargantua/Passes/*.swift) one for one. Structs are the
+ * ShaderTypes.h layouts (gargantua_types.h). Every handle is opaque and owned
+ * by the library; device state (particles, volumes, tables, targets) stays
+ * resident between calls. Host pointers passed in are caller-owned and are
+ * only read or written during the call.
+ *
+ * Errors: every entry point returns a gg_status. Nothing inside the library
+ * exits or traps; gg_last_error() gives one sentence about the most recent
+ * failure on the calling thread. A host maps GG_ERR_INVALID_ARGUMENT to its
+ * usage exit (64) and every other failure to its operational exit (2), as
+ * Sources/Gargantua/Exit.swift:5-18 does.
+ *
+ * Threading: calls on one context are serialised by a mutex inside the
+ * library; all device work of a context is ordered on the context's stream.
+ */
+#ifndef GARGANTUA_H
+#define GARGANTUA_H
+
+#include <stdint.h>
+#include "gargantua_types.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define GG_API __attribute__((visibility("default")))
+
+typedef enum {
+    GG_OK = 0,
+    GG_ERR_INVALID_ARGUMENT = 1,
+    GG_ERR_OUT_OF_MEMORY = 2,
+    GG_ERR_OVER_BUDGET = 3,
+    GG_ERR_DEVICE = 4,
+    GG_ERR_TIMEOUT = 5,
+    GG_ERR_NOT_READY = 6,
+    GG_ERR_NO_DEVICE = 7,
+    GG_ERR_UNSUPPORTED = 8
+} gg_status;
+
+typedef struct gg_context gg_context;
+typedef struct gg_particles gg_particles;
+typedef struct gg_volume gg_volume;
+typedef struct gg_targets gg_targets;
+typedef struct gg_bake gg_bake;
+typedef struct gg_server gg_server;
+
+/* ---------------------------------------------------------------- context */
+
+/* Library version string. Replaces Program.version (Program.swift:5). */
+GG_API const char* gg_version(void);
+
+/* The most recent failure on this thread as one sentence, "" if none. */
+GG_API const char* gg_last_error(void);
+
+/* Name of a status code. */
+GG_API const char* gg_status_name(int status);
+
+/* Open CUDA device `device` with a memory budget. budget_bytes == 0 applies
+ * the reference's rule, min(MEMORY_BUDGET_FRACTION of device memory,
+ * MEMORY_BUDGET_CAP_BYTES) (Budget.swift:6-22); any allocation that would
+ * exceed the budget is refused with GG_ERR_OVER_BUDGET before it is made.
+ * Replaces GpuContext.init (Gpu/GpuContext.swift:7-26) and MemoryBudget. */
+GG_API int gg_context_create(int device, uint64_t budget_bytes, gg_context** out);
+GG_API void gg_context_destroy(gg_context* ctx);
+
+/* Block until every call made on the context has finished on the device. A
+ * device fault reported here is GG_ERR_DEVICE (GpuContext.swift:75-87). */
+GG_API int gg_context_synchronize(gg_context* ctx);
+
+/* Budget accounting: bytes the context may allocate and bytes it holds. */
+GG_API int gg_context_memory(gg_context* ctx, uint64_t* budget, uint64_t* used);
+
+/* The context's CUDA stream (a cudaStream_t), for hosts that order their own
+ * device work with the library's. */
+GG_API void* gg_context_stream(gg_context* ctx);
+
+/* -------------------------------------------------------------- particles */
+
+/* A particle system of `count` particles in device memory, seeded from
+ * `seed`, with its inverse-CDF seeding table (1024 entries, built in FP64 on
+ * the host and rounded to float, DiskModel.swift:54-78) and blackbody colour
+ * table (256 entries, Blackbody.swift:74-82). Replaces ParticleSystem.init
+ * (Sim/ParticleSystem.swift:17-48). potential is PotentialNewtonian or
+ * PotentialPaczynskiWiita. */
+GG_API int gg_particles_create(gg_context* ctx, uint32_t count, uint64_t seed, uint32_t potential,
+                               gg_particles** out);
+GG_API void gg_particles_destroy(gg_particles* ps);
+
+/* The uniforms the particle kernels run with (ParticleSystem.swift:59-70). */
+GG_API int gg_particles_uniforms(gg_particles* ps, SimUniforms* out);
+
+/* Seed every particle from the steady disk profile, event 0. Replaces
+ * SimPass.encodeSeed -> seedParticles (SimPass.swift:24-26, sim.metal:36-42). */
+GG_API int gg_particles_seed(gg_particles* ps);
+
+/* Advance `dispatches` dispatches of SIM_SUBSTEPS substeps each. Replaces
+ * SimPass.encodeStep -> stepParticles (SimPass.swift:28-31, sim.metal:44-79). */
+GG_API int gg_particles_step(gg_particles* ps, uint32_t dispatches);
+
+/* Copy the state out as ShaderTypes Particle records (32 bytes each) into a
+ * host array of `count` entries (count must equal the system's count).
+ * Replaces Validate.readback (Validate.swift:88-100). */
+GG_API int gg_particles_read(gg_particles* ps, Particle* out, uint32_t count);
+
+/* Replace the device state with `count` host Particle records. */
+GG_API int gg_particles_write(gg_particles* ps, const Particle* in, uint32_t count);
+
+/* 64-bit FNV-1a over the AoS bytes of the state (Validate.swift:378-387). */
+GG_API int gg_particles_checksum(gg_particles* ps, uint64_t* out);
+
+/* The float inverse-CDF table the seeding reads (1024 floats). */
+GG_API int gg_particles_inverse_cdf(gg_particles* ps, float* out, uint32_t count);
+
+/* ----------------------------------------------------------------- volume */
+
+/* A size^3 volume: six 32-bit fixed-point sums per voxel and two rgba16f 3-D
+ * textures (emission, velocity). Replaces Volume.init (Gpu/Volume.swift:14-30).
+ * The sums start zeroed. */
+GG_API int gg_volume_create(gg_context* ctx, uint32_t size, gg_volume** out);
+GG_API void gg_volume_destroy(gg_volume* vol);
+
+/* Bin the particles with cloud-in-cell fixed-point atomics, resolve the sums
+ * into the two half-precision textures, and zero the sums, in one call.
+ * u->volumeSize and u->particleCount must match the handles. Replaces
+ * SplatPass.encode (SplatPass.swift:71-76: encodeBin, encodeResolve,
+ * Volume.encodeClear). */
+GG_API int gg_splat(gg_particles* ps, gg_volume* vol, const SplatUniforms* u);
+
+/* The binning alone, leaving the sums in place (SplatPass.encodeBin,
+ * SplatPass.swift:34-49). */
+GG_API int gg_splat_bin(gg_particles* ps, gg_volume* vol, const SplatUniforms* u);
+
+/* The resolve of the current sums into the textures, then zeroing the sums
+ * (SplatPass.encodeResolve + Volume.encodeClear, SplatPass.swift:52-69,
+ * Volume.swift:34-43). */
+GG_API int gg_splat_resolve(gg_volume* vol, const SplatUniforms* u, const gg_particles* ps);
+
+/* Zero the sums (Volume.encodeClear). */
+GG_API int gg_volume_clear(gg_volume* vol);
+
+/* Copy the sums to host arrays in the reference's buffer layouts:
+ * emission u32[2 n^3] (energy, energy*T pairs), momentum i32[3 n^3], mass
+ * u32[n^3], voxel index (z n + y) n + x (splat.metal:21-23). */
+GG_API int gg_volume_read_sums(gg_volume* vol, uint32_t* emission, int32_t* momentum, uint32_t* mass);
+
+/* Copy the resolved textures to host arrays of n^3 half4 (IEEE binary16 bit
+ * patterns, x fastest). Replaces Validate.readVolume (Validate.swift:204-230). */
+GG_API int gg_volume_read(gg_volume* vol, uint16_t* emission_half4, uint16_t* velocity_half4);
+
+/* Upload host half4 textures (n^3 each), e.g. an analytic field for tests. */
+GG_API int gg_volume_write(gg_volume* vol, const uint16_t* emission_half4, const uint16_t* velocity_half4);
+
+/* ------------------------------------------------------ deflection tables */
+
+/* Enable the sphere jump in `inout` for a camera at `camera_radius`: builds
+ * the camera and sky sweep tables for that radius in FP64 on the device (the
+ * sphere table is built once per context), and fills sphereRadius,
+ * cameraRadius, sphereMaxB, sphereTableMaxB, cameraMaxB, skyMinB, skyMaxB.
+ * Replaces DeflectionTables.update + apply (DeflectionTables.swift:57-76). */
+GG_API int gg_tables_update(gg_context* ctx, float camera_radius, MarchUniforms* inout);
+
+/* Copy the three float tables (SWEEP_TABLE_SIZE entries each) to the host;
+ * any pointer may be NULL. */
+GG_API int gg_tables_read(gg_context* ctx, float* sphere, float* camera, float* sky);
+
+/* ------------------------------------------------------------------ march */
+
+/* Render targets of width x height: colour rgba16f, debug rgba16f (drift,
+ * steps, outcome, 1), depth r32f, motion rg16f. Replaces
+ * MarchPass.makeTargets (MarchPass.swift:42-50). */
+GG_API int gg_targets_create(gg_context* ctx, uint32_t width, uint32_t height, gg_targets** out);
+GG_API void gg_targets_destroy(gg_targets* t);
+
+/* Copy targets to host arrays (any pointer may be NULL): colour and debug
+ * as width*height half4, depth as floats, motion as half2. */
+GG_API int gg_targets_read(gg_targets* t, uint16_t* color_half4, uint16_t* debug_half4, float* depth,
+                           uint16_t* motion_half2);
+
+/* Precision policy of the march. */
+typedef enum {
+    /* FP32 RK4 exactly as the reference kernel (march.metal:51-184). */
+    GG_PRECISION_PLAIN = 0,
+    /* FP32 RK4 with compensated (TwoSum) accumulation of the state update
+     * and, for Schwarzschild, rays whose drift exceeds the budget inside
+     * r < 4 re-integrated in FP64. */
+    GG_PRECISION_COMPENSATED = 1
+} gg_precision;
+
+/* March one image (or a tile of it: u->tileOrigin selects the tile, the
+ * targets' size is the tile size) through the volume. vol may be NULL for a
+ * march with no gas. counters may be NULL; when given it is overwritten with
+ * this call's counters. Replaces MarchPass.encodeImage -> marchImage
+ * (MarchPass.swift:103-124, march.metal:194-288). `blackbody` colours come
+ * from the particle system's table; ps may be NULL (stars use the same table,
+ * built on first use). */
+GG_API int gg_march(gg_context* ctx, const gg_volume* vol, const MarchUniforms* u, gg_targets* targets,
+                    int precision, MarchCounters* counters);
+
+/* Integrate `count` probe rays with no gather. Host arrays in and out.
+ * Replaces MarchPass.encodeProbes -> probeRays (MarchPass.swift:148-168,
+ * march.metal:290-341) and Probes.run (Probes.swift:26-43). */
+GG_API int gg_probe(gg_context* ctx, const MarchUniforms* u, const RayProbe* probes, RayProbeResult* results,
+                    uint32_t count, int precision);
+
+/* ------------------------------------------------------------ bake / walk */
+
+/* Bake storage for width x height rays: BAKE_SAMPLES half4 samples per ray
+ * plus a BakedRay header per ray (BakePass.swift:31-38). */
+GG_API int gg_bake_create(gg_context* ctx, uint32_t width, uint32_t height, gg_bake** out);
+GG_API void gg_bake_destroy(gg_bake* b);
+
+/* Bake rows [row_begin, row_end) (u->bakeSpacing, u->bakeCapacity and the
+ * still policy in u->geodesic). Rays over the sample capacity add to the
+ * overflow count. Replaces BakePass.encodeBakeChunk -> bakeRays
+ * (BakePass.swift:55-76, bake.metal:17-92). */
+GG_API int gg_bake_rows(gg_bake* b, const MarchUniforms* u, uint32_t row_begin, uint32_t row_end);
+
+/* Rays of the current bake that overflowed the sample budget; reset with
+ * reset != 0 (BakePass.swift:47-48, 57-60). */
+GG_API int gg_bake_overflow(gg_bake* b, uint32_t* count, int reset);
+
+/* Walk the stored samples through the volume into targets (same size as
+ * the bake). Replaces BakePass.encodeWalk -> walkRays (BakePass.swift:86-102,
+ * bake.metal:94-144). */
+GG_API int gg_walk(gg_bake* b, const gg_volume* vol, const MarchUniforms* u, gg_targets* targets);
+
+/* Copy the baked samples (width*height*BAKE_SAMPLES half4) and headers to
+ * the host; either pointer may be NULL. */
+GG_API int gg_bake_read(gg_bake* b, uint16_t* samples_half4, BakedRay* headers);
+
+/* ------------------------------------------------------------------ present */
+
+/* Tone map the colour target (exposure x HDR -> PBR Neutral -> sRGB
+ * encoding) into width*height*4 bytes of 8-bit sRGB RGBA on the host, or, with
+ * u->debugView != 0, the drift heat map of the debug target. Replaces the
+ * present pass's tonemapFragment (present.metal:22-58) with a headless
+ * buffer in place of the drawable. */
+GG_API int gg_tonemap(gg_targets* t, const PresentUniforms* u, uint8_t* rgba8);
+
+/* Write an 8-bit RGBA image as a PNG file (zlib-compressed, no filter).
+ * Replaces Capture.writePNG (App/Capture.swift:80-94). */
+GG_API int gg_write_png(const char* path, const uint8_t* rgba8, uint32_t width, uint32_t height);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif
