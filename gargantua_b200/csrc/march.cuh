@@ -1,0 +1,369 @@
+// Per-ray march shared by the image, probe, bake and served kernels
+// (march.metal:29-288). Templated on the real type R (float for the march,
+// double for the FP64 re-integration) and on Comp, which accumulates the RK4
+// state update with TwoSum compensation (Knuth 1969, TAOCP vol. 2, 4.2.2):
+// the rounding error of every state += increment is carried in a second
+// word and added back on the next step, which removes the random walk of
+// per-step rounding that dominates FP32 drift over thousands of steps.
+#pragma once
+
+#include "geodesic.cuh"
+#include "kerr.cuh"
+
+namespace gg {
+
+struct MarchParams {
+    MarchUniforms u;
+    SweepTables tables;
+    cudaTextureObject_t emission;  // 0: no gas to gather
+    cudaTextureObject_t velocity;
+    const float4* blackbody;
+    ushort4* color;
+    ushort4* debug;
+    float* depth;
+    ushort2* motion;
+    uint32_t target_width;
+    uint32_t target_height;
+    MarchCounters* counters;
+    unsigned long long* stats;  // ray steps, gather samples, FP64 re-integrated rays
+    uint32_t* flagged;        // FP64 re-integration list (target-local pixel indices)
+    uint32_t* flagged_count;  // its length, a device counter
+    uint32_t flagged_capacity;
+};
+
+struct MarchResult {
+    float3 color;
+    float transmittance;
+    float drift;
+    uint32_t steps;
+    uint32_t outcome;
+    bool leftSphere;
+    float depth;
+    float min_r;
+    uint32_t samples;  // in-slab gather evaluations
+};
+
+// x += y with the error word e carried: TwoSum(x, y + e).
+__device__ __forceinline__ void comp_add(float& x, float& e, float y) {
+    float b = __fadd_rn(y, e);
+    float t = __fadd_rn(x, b);
+    float bp = __fsub_rn(t, x);
+    float ap = __fsub_rn(t, bp);
+    e = __fadd_rn(__fsub_rn(x, ap), __fsub_rn(b, bp));
+    x = t;
+}
+
+template <typename R, bool Comp>
+__device__ __forceinline__ void advance(RayState<R>& s, RayState<R>& c, R h) {
+    RayState<R> inc = ray_increment(s, h);
+    if constexpr (Comp) {
+        comp_add(s.v, c.v, inc.v);
+        comp_add(s.r, c.r, inc.r);
+        comp_add(s.phi, c.phi, inc.phi);
+        comp_add(s.vDot, c.vDot, inc.vDot);
+        comp_add(s.rDot, c.rDot, inc.rDot);
+        comp_add(s.phiDot, c.phiDot, inc.phiDot);
+    } else {
+        s = ray_add(s, inc);
+    }
+}
+
+// Gather one in-slab sample into the running colour (march.metal:81-102).
+__device__ __forceinline__ void gather_sample(const MarchParams& p, float3 position, float f, float3 direction,
+                                              float path, float travelled, float3& color, float& transmittance,
+                                              float& weighted_depth, float& depth_weight, uint32_t& samples) {
+    samples += 1u;
+    Sample s = sample_volume(position, p.u.volumeHalfExtent, p.emission, p.velocity);
+    if (s.density > 0.0f) {
+        float g3 = 1.0f;
+        if (p.u.redshift != 0u) {
+            float g = redshift_factor(f, direction, s.velocity);
+            float gravity = sqrtf(fmaxf(f, 0.0f));
+            float bulk = fminf(s.density / BEAMING_DENSITY_FLOOR, 1.0f);
+            float gr3 = gravity * gravity * gravity;
+            g3 = gr3 + (g * g * g - gr3) * bulk;
+        }
+        float alpha = 1.0f - expf(-p.u.opacityScale * s.density * path);
+        float k = transmittance * g3 * path;
+        float3 contribution = make_float3(s.emission.x * k, s.emission.y * k, s.emission.z * k);
+        color = color + contribution;
+        float weight = dot3(contribution, make_float3(0.2126f, 0.7152f, 0.0722f));
+        weighted_depth += weight * travelled;
+        depth_weight += weight;
+        transmittance *= 1.0f - alpha;
+    }
+}
+
+__device__ __forceinline__ bool in_slab(float3 q, float half_extent) {
+    return fabsf(q.z) < DISK_SLAB_HALF_HEIGHT && fabsf(q.x) < half_extent && fabsf(q.y) < half_extent;
+}
+
+// The Schwarzschild integration loop (march.metal:51-117).
+template <typename R, bool Comp>
+__device__ MarchResult march_ray(const PlaneRay<R>& launched, const MarchParams& p, bool gather, PlaneRay<R>& out) {
+    const MarchUniforms& u = p.u;
+    const GeodesicSettings& g = u.geodesic;
+    PlaneRay<R> ray = launched;
+    RayState<R> comp{};
+    float3 color = make_float3(0.0f, 0.0f, 0.0f);
+    float transmittance = 1.0f;
+    V3<R> previous = ray_position(ray);
+    uint32_t outcome = RayExhausted;
+    bool left_sphere = false;
+    uint32_t steps = 0;
+    float travelled = 0.0f, weighted_depth = 0.0f, depth_weight = 0.0f;
+    uint32_t samples = 0;
+    float min_r = (float)ray.s.r;
+    const R sphere = R(u.sphereRadius);
+    for (uint32_t k = 0; k < STEP_CAP_STILL; ++k) {
+        if (k >= g.stepCap) break;
+        R h = ray_step_length(previous.z, ray.s.r, g);
+        RayState<R> before = ray.s;
+        RayState<R> before_c = comp;
+        advance<R, Comp>(ray.s, comp, h);
+        steps = k + 1u;
+        if (u.sphereRadius > 0.0f && ray.s.r >= sphere && ray.s.rDot > R(0) && before.r < sphere) {
+            // Land on the sphere, where the sweep table is exact (march.metal:71-76).
+            R frac = (sphere - before.r) / (ray.s.r - before.r);
+            ray.s = before;
+            comp = before_c;
+            advance<R, Comp>(ray.s, comp, h * frac);
+        }
+        V3<R> position = ray_position(ray);
+        float path = (float)length(position - previous);
+        travelled += path;
+        min_r = fminf(min_r, (float)ray.s.r);
+        if (ray.s.r <= R(g.captureRadius)) {
+            outcome = RayCaptured;
+            break;
+        }
+        float3 pf = to_float3(position);
+        if (gather && in_slab(pf, u.volumeHalfExtent) && transmittance > 0.004f) {
+            float f = (float)schwarzschild_f(ray.s.r);
+            float3 dir = to_float3(ray_direction(ray));
+            gather_sample(p, pf, f, dir, path, travelled, color, transmittance, weighted_depth, depth_weight, samples);
+        }
+        previous = position;
+        if (u.sphereRadius > 0.0f && ray.s.r >= sphere && ray.s.rDot > R(0)) {
+            outcome = RayEscaped;
+            left_sphere = true;
+            break;
+        }
+        if (ray.s.r >= R(g.escapeRadius)) {
+            outcome = RayEscaped;
+            break;
+        }
+    }
+    out = ray;
+    MarchResult m;
+    m.color = color;
+    m.transmittance = transmittance;
+    if constexpr (Comp) {
+        // Drift of the compensated state, evaluated in double from value +
+        // error word against the launch values evaluated the same way.
+        double r = (double)ray.s.r + (double)comp.r;
+        double e = (1.0 - 2.0 / r) * ((double)ray.s.vDot + (double)comp.vDot) - ((double)ray.s.rDot + (double)comp.rDot);
+        double l = r * r * ((double)ray.s.phiDot + (double)comp.phiDot);
+        double r0 = (double)launched.s.r;
+        double e0 = (1.0 - 2.0 / r0) * (double)launched.s.vDot - (double)launched.s.rDot;
+        double l0 = r0 * r0 * (double)launched.s.phiDot;
+        double ed = fabs(e - e0) / fabs(e0);
+        double ld = fabs(l - l0) / fmax(fabs(l0), 1e-3);
+        m.drift = (float)fmax(ed, ld);
+    } else {
+        m.drift = (float)ray_drift(ray);
+    }
+    m.steps = steps;
+    m.outcome = outcome;
+    m.leftSphere = left_sphere;
+    m.depth = depth_weight > 0.0f ? weighted_depth / depth_weight : travelled;
+    m.min_r = min_r;
+    m.samples = samples;
+    return m;
+}
+
+template <typename R, bool Comp>
+__device__ __forceinline__ void kerr_advance(R a, KerrState<R>& s, KerrVec<R>& c, R h) {
+    KerrVec<R> inc = kerr_increment(a, s, h);
+    if constexpr (Comp) {
+        comp_add(s.r, c.r, inc.r);
+        comp_add(s.theta, c.theta, inc.theta);
+        comp_add(s.phi, c.phi, inc.phi);
+        comp_add(s.pr, c.pr, inc.pr);
+        comp_add(s.ptheta, c.ptheta, inc.ptheta);
+    } else {
+        s.r += inc.r;
+        s.theta += inc.theta;
+        s.phi += inc.phi;
+        s.pr += inc.pr;
+        s.ptheta += inc.ptheta;
+    }
+}
+
+// The Kerr twin of march_ray (march.metal:123-184): no sweep-table jump,
+// capture at the outer horizon plus KERR_CAPTURE_MARGIN, drift = max over
+// steps of the Carter-constant and null-residual gauges.
+template <typename R, bool Comp>
+__device__ MarchResult march_ray_kerr(const KerrState<R>& launched, const MarchParams& p, bool gather, KerrState<R>& out) {
+    const MarchUniforms& u = p.u;
+    const GeodesicSettings& g = u.geodesic;
+    const R a = R(u.spin);
+    KerrState<R> ray = launched;
+    KerrVec<R> comp{};
+    R carter0 = kerr_carter(a, launched);
+    R scale = gmax(gabs(carter0), launched.energy * launched.energy);
+    R capture = kerr_outer_horizon(a) + R(KERR_CAPTURE_MARGIN);
+    float3 color = make_float3(0.0f, 0.0f, 0.0f);
+    float transmittance = 1.0f;
+    V3<R> previous = kerr_position(a, ray);
+    uint32_t outcome = RayExhausted;
+    uint32_t steps = 0;
+    float travelled = 0.0f, weighted_depth = 0.0f, depth_weight = 0.0f;
+    uint32_t samples = 0;
+    R drift = R(0);
+    float min_r = (float)ray.r;
+    for (uint32_t k = 0; k < STEP_CAP_STILL; ++k) {
+        if (k >= g.stepCap) break;
+        kerr_advance<R, Comp>(a, ray, comp, kerr_step_length(a, ray, g));
+        steps = k + 1u;
+        V3<R> position = kerr_position(a, ray);
+        float path = (float)length(position - previous);
+        travelled += path;
+        R cd = gabs(kerr_carter(a, ray) - carter0) / scale;
+        R nd = gabs(kerr_null_residual(a, ray)) / (scale * gmax(ray.r * ray.r, R(1)));
+        drift = gmax(drift, gmax(cd, nd));
+        min_r = fminf(min_r, (float)ray.r);
+        if (ray.r <= capture) {
+            outcome = RayCaptured;
+            break;
+        }
+        float3 pf = to_float3(position);
+        if (gather && in_slab(pf, u.volumeHalfExtent) && transmittance > 0.004f) {
+            R st, ct;
+            gsincos(ray.theta, &st, &ct);
+            float sigma = (float)(ray.r * ray.r + a * a * ct * ct);
+            float fk = 1.0f - 2.0f * (float)ray.r / sigma;
+            float3 dir = to_float3(kerr_direction(a, ray));
+            gather_sample(p, pf, fmaxf(fk, 0.0f), dir, path, travelled, color, transmittance, weighted_depth,
+                          depth_weight, samples);
+        }
+        previous = position;
+        if (ray.r >= R(g.escapeRadius)) {
+            outcome = RayEscaped;
+            break;
+        }
+    }
+    out = ray;
+    MarchResult m;
+    m.color = color;
+    m.transmittance = transmittance;
+    m.drift = (float)drift;
+    m.steps = steps;
+    m.outcome = outcome;
+    m.leftSphere = false;
+    m.depth = depth_weight > 0.0f ? weighted_depth / depth_weight : travelled;
+    m.min_r = min_r;
+    m.samples = samples;
+    return m;
+}
+
+// Falls into the hole: captured, or out of steps moving inward with impact
+// parameter below 3 sqrt 3 (march.metal:44-47).
+template <typename R> __device__ __forceinline__ bool ray_falls_in(const PlaneRay<R>& ray, uint32_t outcome) {
+    return outcome == RayCaptured ||
+           (outcome == RayExhausted && ray.s.rDot < R(0) && gabs(ray.angularMomentum) < R(B_CRITICAL) * ray.energy);
+}
+
+template <typename R>
+__device__ __forceinline__ V3<R> sky_direction(const PlaneRay<R>& ray, const MarchResult& m, const MarchUniforms& u,
+                                               const SweepTables& t) {
+    return m.leftSphere ? sphere_exit_direction(ray, u, t) : ray_direction(ray);
+}
+
+struct PixelResult {
+    float3 color;
+    float drift;
+    uint32_t steps;
+    uint32_t outcome;
+    float depth;
+    float min_r;
+    uint32_t samples;
+};
+
+// Camera ray through a pixel centre plus jitter (march.metal:215-218).
+__device__ __forceinline__ float3 camera_direction(const MarchUniforms& u, uint32_t px, uint32_t py) {
+    float sx = (float)px + 0.5f + u.jitter.x;
+    float sy = (float)py + 0.5f + u.jitter.y;
+    float nx = (2.0f * sx / (float)u.resolution.x - 1.0f) * u.tanHalfFov.x;
+    float ny = (1.0f - 2.0f * sy / (float)u.resolution.y) * u.tanHalfFov.y;
+    return normalize3(to_f3(u.cameraForward) + nx * to_f3(u.cameraRight) + ny * to_f3(u.cameraUp));
+}
+
+// One pixel of marchImage (march.metal:207-273), up to the output writes.
+template <typename R, bool Comp>
+__device__ PixelResult shade_pixel(const MarchParams& p, uint32_t px, uint32_t py) {
+    const MarchUniforms& u = p.u;
+    const bool gather = p.emission != 0;
+    float3 dirf = camera_direction(u, px, py);
+    V3<R> origin = to_v3<R>(to_f3(u.cameraPosition));
+    V3<R> direction = to_v3<R>(dirf);
+    PixelResult r;
+    if (u.spin > 0.0f) {
+        KerrState<R> kray;
+        MarchResult m = march_ray_kerr<R, Comp>(kerr_launch(R(u.spin), origin, direction), p, gather, kray);
+        r.color = m.color;
+        r.drift = m.drift;
+        r.steps = m.steps;
+        r.outcome = m.outcome;
+        r.depth = m.depth;
+        r.min_r = m.min_r;
+        r.samples = m.samples;
+        bool falls_in = m.outcome == RayCaptured || (m.outcome == RayExhausted && kray.pr < R(0));
+        if (!falls_in && u.starBrightness > 0.0f) {
+            float3 star = starfield(to_float3(kerr_direction(R(u.spin), kray)), u.starSeed, p.blackbody);
+            r.color = r.color + star * (m.transmittance * u.starBrightness);
+        }
+        return r;
+    }
+    PreparedRay<R> prepared = prepare_ray(origin, direction, u, p.tables);
+    r.drift = 0.0f;
+    r.steps = 0;
+    r.outcome = RayEscaped;
+    r.depth = 2.0f * R_ESCAPE;
+    r.min_r = (float)prepared.ray.s.r;
+    r.samples = 0;
+    if (prepared.skyOnly) {
+        r.color = u.starBrightness > 0.0f ? starfield(to_float3(prepared.sky), u.starSeed, p.blackbody) * u.starBrightness
+                                          : make_float3(0.0f, 0.0f, 0.0f);
+        return r;
+    }
+    PlaneRay<R> ray;
+    MarchResult m = march_ray<R, Comp>(prepared.ray, p, gather, ray);
+    r.color = m.color;
+    r.drift = m.drift;
+    r.steps = m.steps;
+    r.outcome = m.outcome;
+    r.depth = m.depth;
+    r.min_r = m.min_r;
+    r.samples = m.samples;
+    if (!ray_falls_in(ray, m.outcome) && u.starBrightness > 0.0f) {
+        float3 star = starfield(to_float3(sky_direction(ray, m, u, p.tables)), u.starSeed, p.blackbody);
+        r.color = r.color + star * (m.transmittance * u.starBrightness);
+    }
+    return r;
+}
+
+__device__ __forceinline__ void write_pixel(const MarchParams& p, uint32_t local, const PixelResult& r) {
+    p.color[local] = pack_half4(r.color.x, r.color.y, r.color.z, 1.0f);
+    if (p.debug) p.debug[local] = pack_half4(r.drift, (float)r.steps, (float)r.outcome, 1.0f);
+    if (p.depth) p.depth[local] = fminf(r.depth / (2.0f * R_ESCAPE), 1.0f);
+    if (p.motion) p.motion[local] = make_ushort2(0, 0);
+}
+
+// A ray the compensated FP32 march flags for FP64 re-integration: over the
+// drift budget after passing inside r = 4.
+__device__ __forceinline__ bool needs_fp64(const MarchUniforms& u, const PixelResult& r) {
+    return r.drift > u.driftBudget && r.min_r < 4.0f;
+}
+
+}  // namespace gg

@@ -80,6 +80,11 @@ GG_API int gg_context_memory(gg_context* ctx, uint64_t* budget, uint64_t* used);
  * device work with the library's. */
 GG_API void* gg_context_stream(gg_context* ctx);
 
+/* Copy the blackbody colour table the kernels sample (BLACKBODY_TABLE_SIZE
+ * float4: rgb rounded through half as the reference's rgba16f table, 1) to
+ * the host. The table is Blackbody.table (Blackbody.swift:80-86). */
+GG_API int gg_context_blackbody(gg_context* ctx, float* rgba, uint32_t count);
+
 /* -------------------------------------------------------------- particles */
 
 /* A particle system of `count` particles in device memory, seeded from
@@ -201,6 +206,11 @@ typedef enum {
  * built on first use). */
 GG_API int gg_march(gg_context* ctx, const gg_volume* vol, const MarchUniforms* u, gg_targets* targets,
                     int precision, MarchCounters* counters);
+
+/* Totals of the most recent gg_march on this context: RK4 ray steps (the
+ * `steps` each ray reports, march.metal:70, summed), in-slab gather samples,
+ * and rays re-integrated in FP64. Any pointer may be NULL. */
+GG_API int gg_march_stats(gg_context* ctx, uint64_t* ray_steps, uint64_t* samples, uint64_t* fp64_rays);
 
 /* Integrate `count` probe rays with no gather. Host arrays in and out.
  * Replaces MarchPass.encodeProbes -> probeRays (MarchPass.swift:148-168,

@@ -1,0 +1,111 @@
+"""The C ABI without a GPU: struct layouts, exported symbols, constants, and
+the error path when no device is present."""
+import ctypes as C
+import json
+import os
+import re
+
+import pytest
+
+from conftest import ROOT
+
+HEADER = os.path.join(ROOT, "include", "gargantua.h")
+
+
+def declared_symbols() -> list[str]:
+    names = []
+    for path in sorted(os.listdir(os.path.join(ROOT, "include"))):
+        if path.endswith(".h"):
+            text = open(os.path.join(ROOT, "include", path)).read()
+            names += re.findall(r"GG_API\s+[^;(]*?\b(gg_\w+)\s*\(", text)
+    return names
+
+
+def test_library_exports_every_declared_symbol():
+    import gargantua_b200 as g
+
+    lib = g.lib()
+    names = declared_symbols()
+    assert len(names) >= 40
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_python_signatures_cover_the_header():
+    from gargantua_b200 import _lib
+
+    names = set(declared_symbols())
+    assert names <= set(_lib.SIGNATURES) | {n for n in names if n.startswith("gg_server") or n.endswith("_noalloc")}
+
+
+def test_struct_layouts_match_shadertypes():
+    from gargantua_b200 import types as T
+
+    for struct, size in T.LAYOUT.items():
+        assert C.sizeof(struct) == size, struct.__name__
+    # Offsets ShaderTypes.h produces under Apple simd alignment.
+    assert T.MarchUniforms.cameraRight.offset == 16
+    assert T.MarchUniforms.cameraForward.offset == 48
+    assert T.MarchUniforms.tanHalfFov.offset == 64
+    assert T.MarchUniforms.resolution.offset == 72
+    assert T.MarchUniforms.tileOrigin.offset == 80
+    assert T.MarchUniforms.volumeHalfExtent.offset == 88
+    assert T.MarchUniforms.spin.offset == 148
+    assert T.MarchUniforms.jitter.offset == 152
+    assert T.MarchUniforms.geodesic.offset == 160
+    assert T.SplatUniforms.seed.offset == 32
+    assert T.Particle.temperature.offset == 24
+
+
+def test_c_header_compiles_with_layout_asserts(tmp_path):
+    """The static assertions in gargantua_types.h hold for a C11 and a C++17
+    compiler on this host (the layouts a Swift host sees on Apple)."""
+    import subprocess
+
+    src = tmp_path / "t.c"
+    src.write_text('#include "gargantua.h"\nint main(void){return (int)sizeof(MarchUniforms) - 192;}\n')
+    for cc, std in (("gcc", "-std=c11"), ("g++", "-std=c++17")):
+        exe = tmp_path / ("t_" + cc.replace("+", "p"))
+        r = subprocess.run(["/usr/bin/" + cc, std, "-x", "c" if cc == "gcc" else "c++", str(src), "-I",
+                            os.path.join(ROOT, "include"), "-o", str(exe)], capture_output=True, text=True)
+        assert r.returncode == 0, r.stderr
+        assert subprocess.run([str(exe)]).returncode == 0
+
+
+def test_constants_match_the_reference_table():
+    """Every constant in the reference's generated header carries the same
+    value in include/gargantua_constants.h (StyleTests.swift:40-44 keeps the
+    reference's header equal to its table; this keeps ours equal to theirs)."""
+    with open(os.path.join(ROOT, "tests", "golden", "constants.json")) as fh:
+        ref = json.load(fh)
+    ours = {}
+    text = open(os.path.join(ROOT, "include", "gargantua_constants.h")).read()
+    for m in re.finditer(r"#define\s+([A-Z0-9_]+)\s+\(([-+0-9.eE]+)[fu]\)", text):
+        ours[m.group(1)] = float(m.group(2))
+    assert len(ref) == 53
+    for symbol, value in ref.items():
+        assert symbol in ours, symbol
+        assert ours[symbol] == pytest.approx(value, rel=0, abs=0), symbol
+
+
+def test_every_kernel_loop_names_its_cap():
+    """StyleTests.swift:67-75 carried over: every loop in the device sources
+    is bounded by a named cap or by a size argument."""
+    csrc = os.path.join(ROOT, "gargantua_b200", "csrc")
+    for name in os.listdir(csrc):
+        if name.endswith((".cu", ".cuh")):
+            text = open(os.path.join(csrc, name)).read()
+            assert "while (true)" not in text and "for (;;)" not in text, name
+
+
+def test_context_without_a_device_reports_no_device():
+    import torch
+
+    if torch.cuda.is_available():
+        pytest.skip("a device is present")
+    import gargantua_b200 as g
+
+    with pytest.raises(g.GargantuaError) as e:
+        g.Context()
+    assert e.value.status == 7  # GG_ERR_NO_DEVICE
+    assert "device" in e.value.sentence.lower()
