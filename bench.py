@@ -1,0 +1,428 @@
+"""Benchmark: ray-steps/s of the served, compensated-FP32 march on the mixed
+request stream, against the plain per-request FP32 march; p50/p99 latency.
+
+Workload (one GPU): the served mixed request stream -- still requests with
+Poisson arrivals at 40 req/s, resolution from {320x180, 640x360, 960x540,
+1920x1080, 3840x2160}, step budget from {256, 4096}, spin from {0, 0.5,
+0.9}, camera radius uniform in [40, 120], inclination uniform in [10, 90]
+degrees, azimuth uniform -- all sharing one resident default-preset disk
+(1M particles settled for 600 substeps, exact splat into 128^3). The stream
+is generated from a fixed seed (synthetic data; the reference ships none).
+
+A step serves one slice of `--requests-per-step` consecutive requests of the
+stream, all submitted at once (closed loop), through gg_server_* with pinned
+host output buffers:
+  value  ray steps / device time: the span from the first to the last launch
+         of the step on the device clock (CUDA events), inputs resident;
+  e2e    ray steps / wall time from the first submit to the last result in
+         host memory (device-to-host copies included).
+The plain per-request baseline serves the same slices one request at a time
+through the plain FP32 image kernel. Latency p50/p99 come from a separate
+open-loop replay of the stream's arrivals at 40 req/s.
+
+--impl reference times the reference's CPU path, the FP64 oracle's
+integrators (oracle/, a C restatement of gargantua's Swift oracle), on a
+bounded sample of each slice's rays with every host core.
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+RESOLUTIONS = [(320, 180), (640, 360), (960, 540), (1920, 1080), (3840, 2160)]
+STEP_CAPS = [256, 4096]
+SPINS = [0.0, 0.5, 0.9]
+ARRIVAL_RATE = 40.0
+STREAM_LENGTH = 512
+
+# Algorithmic FP32 operations per unit of work, from running the reference
+# algorithm on a counting scalar type (oracle/opcount.cpp; a CPU test keeps
+# these equal to its output): add/sub/mul/div/sqrt/transcendental = 1.
+FLOPS_SCHWARZSCHILD_STEP = 192  # RK4 165 + position 14 + step policy 3 + path 10
+FLOPS_KERR_STEP = 515           # RK4 436 + step policy, position, path, Carter and null gauges 79
+FLOPS_SAMPLE = 111              # in-slab gather 67 + static-observer direction 44
+
+
+def make_stream(seed: int, count: int = STREAM_LENGTH):
+    """The seeded request stream: arrival time and request parameters."""
+    rng = np.random.default_rng(seed)
+    arrivals = np.cumsum(rng.exponential(1.0 / ARRIVAL_RATE, size=count))
+    out = []
+    for k in range(count):
+        w, h = RESOLUTIONS[rng.integers(len(RESOLUTIONS))]
+        cap = STEP_CAPS[rng.integers(len(STEP_CAPS))]
+        spin = SPINS[rng.integers(len(SPINS))]
+        r = rng.uniform(40.0, 120.0)
+        inclination = math.radians(rng.uniform(10.0, 90.0))
+        azimuth = rng.uniform(0.0, 2.0 * math.pi)
+        out.append({"t": float(arrivals[k]), "width": w, "height": h, "step_cap": cap, "spin": spin,
+                    "distance": float(r), "elevation": math.pi / 2.0 - inclination, "azimuth": float(azimuth),
+                    "seed": seed * 100003 + k})
+    return out
+
+
+def spec_of(q):
+    import gargantua_b200 as g
+
+    return g.RequestSpec(q["width"], q["height"], q["step_cap"], q["spin"], azimuth=q["azimuth"],
+                         elevation=q["elevation"], distance=q["distance"], star_seed=q["seed"])
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device: int):
+        self.device = device
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.device), f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.reader = threading.Thread(target=self._read, daemon=True)
+            self.reader.start()
+        except (OSError, FileNotFoundError):
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.reader.join(timeout=2)
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in self.lines:
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[5:9]):
+                if flag.lower() == "active":
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def flops_of(q, result) -> float:
+    per_step = FLOPS_KERR_STEP if q["spin"] > 0.0 else FLOPS_SCHWARZSCHILD_STEP
+    return float(result.ray_steps) * per_step + float(result.samples) * FLOPS_SAMPLE
+
+
+def serve_slice(server, slice_, pinned):
+    """Submit a slice closed-loop; returns (results, wall seconds, device span
+    seconds, device busy seconds, launches)."""
+    server.totals(reset=True)
+    t0 = time.perf_counter()
+    tickets = [server.submit(spec_of(q), output=out) for q, out in zip(slice_, pinned)]
+    results = [server.wait(t)[2] for t in tickets]
+    wall = time.perf_counter() - t0
+    tot = server.totals(reset=True)
+    return results, wall, tot["span_seconds"], tot["busy_seconds"], tot["launches"]
+
+
+def pinned_outputs(slice_):
+    import torch
+
+    outs = []
+    for q in slice_:
+        t = torch.empty((q["width"] * q["height"], 4), dtype=torch.float16, pin_memory=torch.cuda.is_available())
+        outs.append(t.numpy())
+    return outs
+
+
+def latency_replay(server, stream):
+    """Open loop: submit each request at its arrival time; latency is result
+    ready minus arrival (gg_request_result.finished - submitted)."""
+    pinned = pinned_outputs(stream)
+    t0 = time.perf_counter()
+    base = stream[0]["t"]
+    tickets = []
+    for q, out in zip(stream, pinned):
+        delay = (q["t"] - base) - (time.perf_counter() - t0)
+        if delay > 0:
+            time.sleep(delay)
+        tickets.append(server.submit(spec_of(q), output=out))
+    lat = []
+    for t in tickets:
+        r = server.wait(t)[2]
+        lat.append((r.finished - r.submitted) * 1e3)
+    return float(np.percentile(lat, 50)), float(np.percentile(lat, 99))
+
+
+def cpu_sample(slices, seconds: float, threads: int):
+    """The oracle's FP64 integrators on a bounded sample of the slices' rays:
+    returns (ray steps per second, rays, steps, seconds, description)."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_ffi as O
+
+    import gargantua_b200 as g
+
+    rng = np.random.default_rng(7)
+    total_steps, total_rays, elapsed = 0, 0, 0.0
+    per_request = 256
+    flat = [q for s in slices for q in s]
+    k = 0
+    while elapsed < seconds and k < 4 * len(flat):
+        q = flat[k % len(flat)]
+        k += 1
+        cam = g.OrbitCamera(q["azimuth"], q["elevation"], q["distance"])
+        launches = g.camera_grid(cam, 64, 36, q["width"] / q["height"])
+        pick = rng.choice(len(launches), size=min(per_request, len(launches)), replace=False)
+        probes = np.array([np.concatenate([launches[i].origin, launches[i].direction]) for i in pick])
+        escape = max(60.0, q["distance"] + 10.0)
+        t0 = time.perf_counter()
+        if q["spin"] > 0.0:
+            st = O.KerrSettings(0.02, 0.005, 0.5, 0.05, escape, q["step_cap"])
+            res = O.kerr_integrate_batch(q["spin"], probes, st, threads)
+        else:
+            interactive = q["step_cap"] <= 256
+            st = O.Settings(0.02, 0.02, 0.5, 2.02, escape, q["step_cap"], 0.1 if interactive else 0.06,
+                            3.0 if interactive else 1.5)
+            res = O.integrate_batch(probes, st, threads)
+        elapsed += time.perf_counter() - t0
+        total_steps += int(res[:, 8].sum())
+        total_rays += len(probes)
+    desc = (f"FP64 oracle integrators, {total_rays} rays ({per_request} per request from a 64x36 grid of each "
+            f"request's camera) over {k} requests of the timed slices, {threads} threads")
+    return total_steps / max(elapsed, 1e-9), total_rays, total_steps, elapsed, desc
+
+
+def setup_world(device: int):
+    import gargantua_b200 as g
+
+    # A server-sized budget: the reference's 3 GB cap is a laptop rule.
+    ctx = g.Context(device, budget_bytes=48 << 30)
+    ps = g.Particles(ctx, 1_000_000, seed=1)
+    ps.advance(300, seed_first=True)  # STILL_SETTLE_STEPS = 600 substeps
+    vol = g.Volume(ctx, 128)
+    vol.splat(ps, exact=True)
+    ctx.synchronize()
+    return ctx, ps, vol
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=8)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--requests-per-step", type=int, default=32)
+    ap.add_argument("--latency-requests", type=int, default=48)
+    ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    args = ap.parse_args()
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    B = args.requests_per_step
+    nslices = args.warmup + args.steps
+
+    if args.impl == "reference":
+        # The reference's CPU path on rank 0 only; other ranks do no work.
+        if rank != 0:
+            return
+        threads = os.cpu_count() or 1
+        stream = make_stream(1)
+        slices = [stream[i * B:(i + 1) * B] for i in range(nslices)]
+        budget = max(3.0, args.cpu_seconds / 2)
+        for s in slices[:args.warmup]:
+            cpu_sample([s], 0.2, threads)
+        vals, steps_total, secs_total, rays_total = [], 0, 0.0, 0
+        for s in slices[args.warmup:]:
+            v, rays, steps, secs, desc = cpu_sample([s], budget / max(args.steps, 1), threads)
+            vals.append(v)
+            steps_total += steps
+            secs_total += secs
+            rays_total += rays
+        value = steps_total / secs_total
+        line = {
+            "metric": "ray-steps/s, served mixed request stream (4096-step E/L drift < 1e-5), p50/p99 ms",
+            "value": value, "unit": "ray-steps/s", "impl": "reference", "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * secs_total / max(args.steps, 1), "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": {"workload": "served mixed request stream, 40 req/s Poisson, 1M-particle 128^3 disk",
+                       "requests_per_step": B, "stream_seed": 1},
+            "cpu_baseline": {"value": value, "unit": "ray-steps/s", "cores": threads, "kind": "port",
+                             "sample": desc},
+            "e2e": {"value": value, "unit": "ray-steps/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        }
+        print(json.dumps(line))
+        return
+
+    import torch
+
+    dist = None
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    import gargantua_b200 as g
+
+    ctx, ps, vol = setup_world(local)
+    peak = ctx.fp32_peak_tflops()
+    # Weak scaling: every rank serves its own stream (seed 1 + rank).
+    stream = make_stream(1 + rank)
+    slices = [stream[i * B:(i + 1) * B] for i in range(nslices)]
+    batched = g.Server(ctx, vol, g.types.SERVE_BATCHED)
+
+    def barrier():
+        torch.cuda.synchronize()
+        if dist is not None:
+            dist.barrier()
+
+    for s in slices[:args.warmup]:
+        serve_slice(batched, s, pinned_outputs(s))
+    timed = slices[args.warmup:]
+    pins = [pinned_outputs(s) for s in timed]
+    clocks = ClockSampler(local)
+    barrier()
+    clocks.start()
+    span = busy = wall = 0.0
+    steps_total = flops_total = 0.0
+    launches = 0
+    d2h = 0
+    schw_requests = 0
+    drift_over = rays_total = 0
+    for s, pin in zip(timed, pins):
+        results, w, sp, bu, la = serve_slice(batched, s, pin)
+        wall += w
+        span += sp
+        busy += bu
+        launches += la
+        for q, r in zip(s, results):
+            steps_total += r.ray_steps
+            flops_total += flops_of(q, r)
+            d2h += q["width"] * q["height"] * 8
+            schw_requests += 1 if q["spin"] == 0.0 else 0
+            rays_total += r.counters.rays
+            drift_over += r.counters.overDriftBudget
+    barrier()
+    clock_info = clocks.stop()
+
+    def max_over_ranks(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    def sum_over_ranks(x):
+        if dist is None:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+        return float(t.item())
+
+    span_max = max_over_ranks(span)
+    wall_max = max_over_ranks(wall)
+    steps_all = sum_over_ranks(steps_total)
+    value = steps_all / span_max
+    e2e = steps_all / wall_max
+
+    # The plain per-request baseline on the same slices.
+    plain = None
+    if not args.no_plain:
+        server_plain = g.Server(ctx, vol, g.types.SERVE_SERIAL_PLAIN)
+        serve_slice(server_plain, slices[0], pinned_outputs(slices[0]))
+        barrier()
+        p_span = p_wall = p_steps = 0.0
+        for s, pin in zip(timed, pins):
+            results, w, sp, bu, la = serve_slice(server_plain, s, pin)
+            p_span += sp
+            p_wall += w
+            p_steps += sum(r.ray_steps for r in results)
+        barrier()
+        p_span, p_wall, p_steps = max_over_ranks(p_span), max_over_ranks(p_wall), sum_over_ranks(p_steps)
+        plain = {"value": p_steps / p_span, "e2e": p_steps / p_wall, "unit": "ray-steps/s",
+                 "served_over_plain": value / (p_steps / p_span),
+                 "served_over_plain_e2e": e2e / (p_steps / p_wall)}
+        lat_stream = stream[nslices * B:nslices * B + args.latency_requests]
+        if len(lat_stream) >= 8:
+            plain["p50_ms"], plain["p99_ms"] = latency_replay(server_plain, lat_stream)
+        server_plain.close()
+
+    lat_stream = stream[nslices * B:nslices * B + args.latency_requests]
+    p50 = p99 = None
+    if len(lat_stream) >= 8:
+        p50, p99 = latency_replay(batched, lat_stream)
+
+    cpu = None
+    if rank == 0 and world == 1:
+        threads = os.cpu_count() or 1
+        cv, crays, csteps, csecs, desc = cpu_sample(timed, args.cpu_seconds, threads)
+        cpu = {"value": cv, "unit": "ray-steps/s", "cores": threads, "kind": "port", "sample": desc}
+
+    achieved = flops_total / busy / 1e12
+    line = {
+        "metric": "ray-steps/s, served mixed request stream (4096-step E/L drift < 1e-5), p50/p99 ms",
+        "value": value,
+        "unit": "ray-steps/s",
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": 1e3 * span_max / args.steps,
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f32",
+        "data": "synthetic",
+        "config": {"workload": "served mixed request stream (configs: 40 req/s Poisson; 320x180..3840x2160; "
+                               "256/4096 steps; spin 0/0.5/0.9; r 40-120; 1M-particle settled disk, 128^3)",
+                   "requests_per_step": B, "stream_seed": 1, "precision": "compensated FP32 + FP64 re-integration",
+                   "l2": "inputs larger than L2 (outputs up to 66 MB per request, 8-200 MB per step)"},
+        "p50_ms": p50,
+        "p99_ms": p99,
+        "plain_per_request": plain,
+        "drift": {"rays": rays_total, "over_budget": drift_over},
+        "e2e": {"value": e2e, "unit": "ray-steps/s", "h2d_bytes_per_step": int(B * 64),
+                "d2h_bytes_per_step": int(d2h / max(args.steps, 1))},
+        "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
+                     "frac": achieved / peak, "traffic": None,
+                     "peak_source": "measured FP32 FMA microbenchmark (gg_measure_fp32_peak) on this GPU",
+                     "kernel": "serve_kernel (persistent, work-stealing)"},
+        "cpu_baseline": cpu,
+        "clocks": clock_info,
+        "gpu_launches": int(launches * 2 + schw_requests * 2),
+    }
+    batched.close()
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line))
+
+
+if __name__ == "__main__":
+    main()

@@ -90,6 +90,13 @@ SIGNATURES = {
     "gg_bake_read": (i, [vp, vp, vp]),
     "gg_tonemap": (i, [vp, P(T.PresentUniforms), vp]),
     "gg_write_png": (i, [C.c_char_p, vp, u32, u32]),
+    "gg_server_create": (i, [vp, vp, P(T.ServerConfig), P(vp)]),
+    "gg_server_destroy": (None, [vp]),
+    "gg_server_submit": (i, [vp, P(T.Request), P(u64)]),
+    "gg_server_poll": (i, [vp, u64, P(i)]),
+    "gg_server_wait": (i, [vp, u64, C.c_double, P(T.RequestResult)]),
+    "gg_server_totals": (i, [vp, i, P(u64), P(u64), P(u64), P(C.c_double), P(C.c_double)]),
+    "gg_measure_fp32_peak": (i, [vp, P(C.c_double)]),
 }
 
 

@@ -7,7 +7,7 @@
 // list that a second kernel re-integrates in FP64.
 #include <vector>
 
-#include "march.cuh"
+#include "lanes.cuh"
 #include "runtime.h"
 
 namespace gg {
@@ -22,7 +22,7 @@ __global__ void __launch_bounds__(64) march_image_kernel(MarchParams p) {
     PixelResult r{};
     r.outcome = RayEscaped;
     if (active) {
-        r = shade_pixel<float, Comp>(p, px, py);
+        r = Comp ? shade_pixel_compensated(p, px, py) : shade_pixel<float, false>(p, px, py);
         const uint32_t local = gy * p.target_width + gx;
         write_pixel(p, local, r);
         if (Comp && p.flagged && needs_fp64(p.u, r)) {
@@ -122,8 +122,34 @@ __global__ void __launch_bounds__(64) probe_kernel(MarchParams p, const RayProbe
     if (i >= count) return;
     RayProbe q = probes[i];
     float min_r = 0.0f;
-    RayProbeResult r = probe_one<float, Comp>(p, q, &min_r);
-    if (Comp && r.drift > p.u.driftBudget && min_r < 4.0f) r = probe_one<double, false>(p, q, &min_r);
+    RayProbeResult r;
+    if (Comp) {
+        const MarchUniforms& u = p.u;
+        float3 origin = make_float3(q.origin.x, q.origin.y, q.origin.z);
+        float3 dir = make_float3(q.direction.x, q.direction.y, q.direction.z);
+        if (u.spin > 0.0f) {
+            KLane l;
+            k_init(l, origin, dir, u);
+            for (uint32_t k = 0; k <= STEP_CAP_STILL; ++k)
+                if (k_step(l, u, 0, 0, false)) break;
+            r = k_probe_result(l);
+            min_r = l.min_r;
+        } else {
+            SLane l;
+            float3 sky;
+            if (s_init(l, origin, dir, u, p.tables, &sky)) {
+                r = probe_one<float, false>(p, q, &min_r);  // sky-only: no integration either way
+            } else {
+                for (uint32_t k = 0; k <= STEP_CAP_STILL; ++k)
+                    if (s_step(l, u, 0, 0, false)) break;
+                r = s_probe_result(l, u, p.tables);
+                min_r = l.min_r;
+            }
+        }
+        if (r.drift > u.driftBudget && min_r < 4.0f) r = probe_one<double, false>(p, q, &min_r);
+    } else {
+        r = probe_one<float, false>(p, q, &min_r);
+    }
     results[i] = r;
 }
 
@@ -137,6 +163,13 @@ MarchParams make_params(gg_context* ctx, const gg_volume* vol, const MarchUnifor
     p.velocity = vol ? vol->velocity_tex : 0;
     p.blackbody = ctx->blackbody;
     return p;
+}
+
+int launch_plain_image(const MarchParams& p, cudaStream_t stream) {
+    dim3 block(MARCH_THREADGROUP_WIDTH, MARCH_THREADGROUP_HEIGHT);
+    dim3 grid((p.target_width + block.x - 1) / block.x, (p.target_height + block.y - 1) / block.y);
+    march_image_kernel<false><<<grid, block, 0, stream>>>(p);
+    return launch_status("plain march");
 }
 
 // The tables the uniforms enable must exist: sphereRadius > 0 means the

@@ -68,22 +68,34 @@ __device__ __forceinline__ void advance(RayState<R>& s, RayState<R>& c, R h) {
     }
 }
 
+struct GatherView {
+    cudaTextureObject_t emission;
+    cudaTextureObject_t velocity;
+    float half_extent;
+    float opacity;
+    uint32_t redshift;
+};
+
+__device__ __forceinline__ GatherView gather_view(const MarchUniforms& u, cudaTextureObject_t em, cudaTextureObject_t vel) {
+    return GatherView{em, vel, u.volumeHalfExtent, u.opacityScale, u.redshift};
+}
+
 // Gather one in-slab sample into the running colour (march.metal:81-102).
-__device__ __forceinline__ void gather_sample(const MarchParams& p, float3 position, float f, float3 direction,
+__device__ __forceinline__ void gather_sample(const GatherView& gv, float3 position, float f, float3 direction,
                                               float path, float travelled, float3& color, float& transmittance,
                                               float& weighted_depth, float& depth_weight, uint32_t& samples) {
     samples += 1u;
-    Sample s = sample_volume(position, p.u.volumeHalfExtent, p.emission, p.velocity);
+    Sample s = sample_volume(position, gv.half_extent, gv.emission, gv.velocity);
     if (s.density > 0.0f) {
         float g3 = 1.0f;
-        if (p.u.redshift != 0u) {
+        if (gv.redshift != 0u) {
             float g = redshift_factor(f, direction, s.velocity);
             float gravity = sqrtf(fmaxf(f, 0.0f));
             float bulk = fminf(s.density / BEAMING_DENSITY_FLOOR, 1.0f);
             float gr3 = gravity * gravity * gravity;
             g3 = gr3 + (g * g * g - gr3) * bulk;
         }
-        float alpha = 1.0f - expf(-p.u.opacityScale * s.density * path);
+        float alpha = 1.0f - expf(-gv.opacity * s.density * path);
         float k = transmittance * g3 * path;
         float3 contribution = make_float3(s.emission.x * k, s.emission.y * k, s.emission.z * k);
         color = color + contribution;
@@ -141,7 +153,8 @@ __device__ MarchResult march_ray(const PlaneRay<R>& launched, const MarchParams&
         if (gather && in_slab(pf, u.volumeHalfExtent) && transmittance > 0.004f) {
             float f = (float)schwarzschild_f(ray.s.r);
             float3 dir = to_float3(ray_direction(ray));
-            gather_sample(p, pf, f, dir, path, travelled, color, transmittance, weighted_depth, depth_weight, samples);
+            gather_sample(gather_view(u, p.emission, p.velocity), pf, f, dir, path, travelled, color, transmittance, weighted_depth,
+                          depth_weight, samples);
         }
         previous = position;
         if (u.sphereRadius > 0.0f && ray.s.r >= sphere && ray.s.rDot > R(0)) {
@@ -244,8 +257,8 @@ __device__ MarchResult march_ray_kerr(const KerrState<R>& launched, const MarchP
             float sigma = (float)(ray.r * ray.r + a * a * ct * ct);
             float fk = 1.0f - 2.0f * (float)ray.r / sigma;
             float3 dir = to_float3(kerr_direction(a, ray));
-            gather_sample(p, pf, fmaxf(fk, 0.0f), dir, path, travelled, color, transmittance, weighted_depth,
-                          depth_weight, samples);
+            gather_sample(gather_view(u, p.emission, p.velocity), pf, fmaxf(fk, 0.0f), dir, path, travelled, color,
+                          transmittance, weighted_depth, depth_weight, samples);
         }
         previous = position;
         if (ray.r >= R(g.escapeRadius)) {

@@ -1,0 +1,853 @@
+// Serving: continuous batching of still requests onto the device.
+//
+// Device side. A wave is one persistent launch over a queue of ray chunks
+// (chunk_rays consecutive pixels of one request) packed from every admitted
+// request, with one queue per metric: Schwarzschild rays and Kerr rays run
+// different integrators, so a warp works one queue at a time (half the
+// warps start on each, then take the other). Each warp steals chunks with
+// one atomic per chunk and keeps its 32 lanes busy: a lane whose ray ended
+// is refilled from the warp's chunk (ballot + popc ranks the idle lanes) as
+// soon as a quarter of the warp is idle, so long and short rays share warps
+// without the 8x8-tile tail of the per-request kernel. Ray state stays in
+// registers for the whole ray. Per-request counters are aggregated across
+// the lanes of a warp that finish together (match_any + reduce) before one
+// atomic per request. Rays over their drift budget after passing inside
+// r = 4 are queued for an FP64 re-integration kernel that runs after the
+// wave. The wave (counter reset, persistent kernel, FP64 pass) is captured
+// once per slot into a CUDA graph and replayed; only the wave's descriptors
+// are copied in before each replay.
+//
+// Host side. A scheduler thread admits submitted requests in arrival order
+// while their device footprint fits the server's memory (the HBM admission
+// the reference's MemoryBudget does before allocating, Budget.swift:6-22),
+// builds their sweep tables in FP64 on a side stream, forms waves
+// round-robin across admitted requests (so a small request that arrives
+// behind a large one is packed into the next wave rather than queued behind
+// it), keeps up to max_waves_in_flight waves on alternating streams so one
+// wave's tail overlaps the next wave's start, and copies each finished
+// request's pixels to its host buffer on a copy stream.
+#include <algorithm>
+#include <atomic>
+#include <chrono>
+#include <condition_variable>
+#include <cstring>
+#include <deque>
+#include <map>
+#include <memory>
+#include <thread>
+#include <vector>
+
+#include "lanes.cuh"
+#include "runtime.h"
+
+namespace gg {
+
+MarchParams make_params(gg_context* ctx, const gg_volume* vol, const MarchUniforms& u, const gg_sweep* sweep);
+int launch_plain_image(const MarchParams& p, cudaStream_t stream);
+
+struct ServeRequest {
+    MarchUniforms u;
+    const float* camera_table;
+    const float* sky_table;
+    ushort4* color;
+    ushort4* debug;
+    unsigned long long* stats;  // steps, samples, fp64, rays, over budget, exhausted, captured, spare
+    uint32_t pad[6];
+};
+static_assert(sizeof(ServeRequest) == 256, "ServeRequest");
+
+struct ServeChunk {
+    uint32_t request, first, count, pad;
+};
+
+struct WaveHeader {
+    uint32_t chunk_count[2];
+    uint32_t heads[2];
+    uint32_t flagged_count;
+    uint32_t request_count;
+    uint32_t pad[10];
+};
+static_assert(sizeof(WaveHeader) == 64, "WaveHeader");
+
+struct WaveArgs {
+    WaveHeader* header;
+    const ServeRequest* requests;
+    const ServeChunk* chunks0;
+    const ServeChunk* chunks1;
+    unsigned long long* flagged;
+    uint32_t flagged_capacity;
+    const float* sphere_table;
+    const float4* blackbody;
+    cudaTextureObject_t emission;
+    cudaTextureObject_t velocity;
+};
+
+constexpr unsigned kFull = 0xffffffffu;
+constexpr int kStepsPerRound = 8;       // RK4 steps between refill checks
+constexpr int kRefillIdle = 8;          // refill once this many lanes are idle
+constexpr uint32_t kMaxRounds = 1u << 28;  // bound on a warp's rounds (each consumes work or a step)
+constexpr uint32_t kMaxFillsPerRound = 64;
+constexpr int kServeThreads = 128;
+
+__device__ __forceinline__ void write_result(const ServeRequest& R, uint32_t pixel, const PixelResult& r) {
+    R.color[pixel] = pack_half4(r.color.x, r.color.y, r.color.z, 1.0f);
+    if (R.debug) R.debug[pixel] = pack_half4(r.drift, (float)r.steps, (float)r.outcome, 1.0f);
+}
+
+// Warp-aggregated per-request counters for the lanes that finished a ray
+// this iteration. Every lane of the warp calls it.
+__device__ __forceinline__ void account(const WaveArgs& a, bool finished, uint32_t req, const PixelResult& r,
+                                        float budget, uint32_t lane) {
+    unsigned fin = __ballot_sync(kFull, finished);
+    if (!finished) return;
+    unsigned peers = __match_any_sync(fin, req);
+    uint32_t steps = __reduce_add_sync(peers, r.steps);
+    uint32_t samples = __reduce_add_sync(peers, r.samples);
+    uint32_t rays = __popc(peers);
+    uint32_t over = __reduce_add_sync(peers, r.drift > budget ? 1u : 0u);
+    uint32_t exhausted = __reduce_add_sync(peers, r.outcome == RayExhausted ? 1u : 0u);
+    uint32_t captured = __reduce_add_sync(peers, r.outcome == RayCaptured ? 1u : 0u);
+    if ((int)lane == __ffs(peers) - 1) {
+        unsigned long long* st = a.requests[req].stats;
+        if (steps) atomicAdd(st + 0, (unsigned long long)steps);
+        if (samples) atomicAdd(st + 1, (unsigned long long)samples);
+        atomicAdd(st + 3, (unsigned long long)rays);
+        if (over) atomicAdd(st + 4, (unsigned long long)over);
+        if (exhausted) atomicAdd(st + 5, (unsigned long long)exhausted);
+        if (captured) atomicAdd(st + 6, (unsigned long long)captured);
+    }
+}
+
+// Write a finished ray, or queue it for FP64 re-integration.
+__device__ __forceinline__ void complete(const WaveArgs& a, uint32_t req, uint32_t pixel, const PixelResult& r) {
+    const ServeRequest& R = a.requests[req];
+    if (needs_fp64(R.u, r)) {
+        uint32_t slot = atomicAdd(&a.header->flagged_count, 1u);
+        if (slot < a.flagged_capacity) {
+            a.flagged[slot] = ((unsigned long long)req << 32) | pixel;
+            return;
+        }
+    }
+    write_result(R, pixel, r);
+}
+
+template <int Kind> struct LaneOf;
+template <> struct LaneOf<0> { typedef SLane type; };
+template <> struct LaneOf<1> { typedef KLane type; };
+
+template <int Kind>
+__device__ void serve_queue(const WaveArgs& a, uint32_t lane) {
+    const ServeChunk* chunks = Kind == 0 ? a.chunks0 : a.chunks1;
+    const uint32_t nchunks = a.header->chunk_count[Kind];
+    uint32_t* head = &a.header->heads[Kind];
+    const bool gather = a.emission != 0;
+    const unsigned lower = (1u << lane) - 1u;
+    typename LaneOf<Kind>::type L;
+    bool active = false;
+    uint32_t req = 0, pixel = 0;
+    uint32_t cursor = 0, chunk_end = 0, chunk_req = 0;
+    bool drained = false;
+    for (uint32_t round = 0; round < kMaxRounds; ++round) {
+        // Refill idle lanes from the warp's chunk, stealing new chunks.
+        for (uint32_t fill = 0; fill < kMaxFillsPerRound && !drained; ++fill) {
+            unsigned idle = __ballot_sync(kFull, !active);
+            if (idle == 0u) break;
+            if (cursor >= chunk_end) {
+                uint32_t c = 0;
+                if (lane == 0) c = atomicAdd(head, 1u);
+                c = __shfl_sync(kFull, c, 0);
+                if (c >= nchunks) {
+                    drained = true;
+                    break;
+                }
+                ServeChunk ch = chunks[c];
+                cursor = ch.first;
+                chunk_end = ch.first + ch.count;
+                chunk_req = ch.request;
+            }
+            uint32_t take = min((uint32_t)__popc(idle), chunk_end - cursor);
+            uint32_t rank = __popc(idle & lower);
+            bool sky_done = false;
+            PixelResult r{};
+            if (!active && rank < take) {
+                req = chunk_req;
+                pixel = cursor + rank;
+                const ServeRequest& R = a.requests[req];
+                uint32_t w = R.u.resolution.x;
+                float3 dir = camera_direction(R.u, pixel % w, pixel / w);
+                float3 origin = to_f3(R.u.cameraPosition);
+                if constexpr (Kind == 0) {
+                    float3 sky;
+                    SweepTables t{a.sphere_table, R.camera_table, R.sky_table};
+                    if (s_init(L, origin, dir, R.u, t, &sky)) {
+                        r = sky_only_result(sky, R.u, a.blackbody);
+                        write_result(R, pixel, r);
+                        sky_done = true;
+                    } else {
+                        active = true;
+                    }
+                } else {
+                    k_init(L, origin, dir, R.u);
+                    active = true;
+                }
+            }
+            account(a, sky_done, req, r, 1e30f, lane);
+            cursor += take;
+        }
+        unsigned act = __ballot_sync(kFull, active);
+        if (act == 0u) {
+            if (drained) break;
+            continue;
+        }
+        // Advance every active lane, a few steps per round.
+        for (int it = 0; it < kStepsPerRound; ++it) {
+            bool finished = false;
+            PixelResult r{};
+            float budget = 0.0f;
+            if (active) {
+                const ServeRequest& R = a.requests[req];
+                if constexpr (Kind == 0) {
+                    finished = s_step(L, R.u, a.emission, a.velocity, gather);
+                    if (finished) {
+                        SweepTables t{a.sphere_table, R.camera_table, R.sky_table};
+                        r = s_finish(L, R.u, t, a.blackbody);
+                    }
+                } else {
+                    finished = k_step(L, R.u, a.emission, a.velocity, gather);
+                    if (finished) r = k_finish(L, R.u, a.blackbody);
+                }
+                budget = R.u.driftBudget;
+                if (finished) {
+                    complete(a, req, pixel, r);
+                    active = false;
+                }
+            }
+            account(a, finished, req, r, budget, lane);
+            act = __ballot_sync(kFull, active);
+            if (act == 0u) break;
+            if (!drained && __popc(~act) >= kRefillIdle) break;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(kServeThreads) serve_kernel(WaveArgs a) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    if (warp & 1u) {
+        serve_queue<1>(a, lane);
+        serve_queue<0>(a, lane);
+    } else {
+        serve_queue<0>(a, lane);
+        serve_queue<1>(a, lane);
+    }
+}
+
+// FP64 re-integration of the wave's flagged rays.
+__global__ void __launch_bounds__(128) serve_reintegrate_kernel(WaveArgs a) {
+    const uint32_t n = min(a.header->flagged_count, a.flagged_capacity);
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        unsigned long long e = a.flagged[i];
+        uint32_t req = (uint32_t)(e >> 32), pixel = (uint32_t)e;
+        const ServeRequest& R = a.requests[req];
+        MarchParams p{};
+        p.u = R.u;
+        p.tables = SweepTables{a.sphere_table, R.camera_table, R.sky_table};
+        p.emission = a.emission;
+        p.velocity = a.velocity;
+        p.blackbody = a.blackbody;
+        uint32_t w = R.u.resolution.x;
+        PixelResult r = shade_pixel<double, false>(p, pixel % w, pixel / w);
+        write_result(R, pixel, r);
+        atomicAdd(R.stats + 2, 1ull);
+    }
+}
+
+// ------------------------------------------------------------------- host
+
+static double now_seconds() {
+    using namespace std::chrono;
+    return duration<double>(steady_clock::now().time_since_epoch()).count();
+}
+
+// MarchPass.uniforms (MarchPass.swift:67-98) for a request, with the orbit
+// camera's basis in float as Camera.swift computes it.
+static MarchUniforms request_uniforms(const gg_request& q) {
+    MarchUniforms u{};
+    float c = cosf(q.elevation);
+    float px = q.distance * (c * cosf(q.azimuth)), py = q.distance * (c * sinf(q.azimuth)), pz = q.distance * sinf(q.elevation);
+    float inv = 1.0f / sqrtf(px * px + py * py + pz * pz);
+    float fx = -px * inv, fy = -py * inv, fz = -pz * inv;
+    // right = normalize(cross(forward, z)), up = cross(right, forward)
+    float rx = fy, ry = -fx, rz = 0.0f;
+    float rn = 1.0f / sqrtf(rx * rx + ry * ry);
+    rx *= rn;
+    ry *= rn;
+    float ux = ry * fz - rz * fy, uy = rz * fx - rx * fz, uz = rx * fy - ry * fx;
+    u.cameraPosition = {px, py, pz, 0.0f};
+    u.cameraRight = {rx, ry, rz, 0.0f};
+    u.cameraUp = {ux, uy, uz, 0.0f};
+    u.cameraForward = {fx, fy, fz, 0.0f};
+    float t = tanf(q.fov_y * 0.5f);
+    u.tanHalfFov = {t * (float)q.width / (float)q.height, t};
+    u.resolution = {q.width, q.height};
+    u.tileOrigin = {0u, 0u};
+    u.volumeHalfExtent = VOLUME_HALF_EXTENT;
+    u.opacityScale = VOLUME_OPACITY;
+    u.starBrightness = (q.flags & GG_REQUEST_NO_STARS) ? 0.0f : STAR_BRIGHTNESS;
+    const bool interactive = q.step_cap <= STEP_CAP_INTERACTIVE;
+    u.driftBudget = interactive ? DRIFT_BUDGET_INTERACTIVE : DRIFT_BUDGET_STILL;
+    u.starSeed = q.star_seed;
+    u.redshift = (q.flags & GG_REQUEST_NO_REDSHIFT) ? 0u : 1u;
+    u.bakeSpacing = 0.0f;
+    u.bakeCapacity = BAKE_SAMPLES;
+    u.spin = q.spin;
+    u.jitter = {0.0f, 0.0f};
+    GeodesicSettings& g = u.geodesic;
+    g.stepFactor = STEP_RADIUS_FACTOR;
+    g.stepMin = STEP_MIN;
+    g.stepMax = STEP_MAX;
+    g.captureRadius = R_CAPTURE;
+    g.escapeRadius = R_ESCAPE;
+    // Kerr has no sphere jump; a camera beyond R_ESCAPE would escape on its
+    // first step, so its escape radius moves out with it.
+    if (q.spin > 0.0f) g.escapeRadius = fmaxf(R_ESCAPE, q.distance + 10.0f);
+    g.stepCap = q.step_cap;
+    g.emptyStepFactor = interactive ? STEP_FACTOR_EMPTY_INTERACTIVE : STEP_FACTOR_EMPTY_STILL;
+    g.emptyStepMax = interactive ? STEP_MAX_EMPTY_INTERACTIVE : STEP_MAX_EMPTY_STILL;
+    return u;
+}
+
+struct ServedRequest {
+    uint64_t ticket = 0;
+    gg_request q{};
+    MarchUniforms u{};
+    gg_sweep sweep;
+    ushort4* d_color = nullptr;
+    ushort4* d_debug = nullptr;
+    unsigned long long* d_stats = nullptr;  // 8 u64 then a MarchCounters
+    uint64_t footprint = 0;
+    uint32_t rays = 0;
+    uint32_t next_ray = 0;
+    int waves_pending = 0;
+    bool copying = false;
+    bool done = false;
+    cudaEvent_t copied = nullptr;
+    unsigned long long host_stats[10] = {};
+    gg_request_result result{};
+};
+
+struct WaveSlot {
+    cudaStream_t stream = nullptr;
+    cudaEvent_t start = nullptr, stop = nullptr;
+    cudaGraphExec_t graph = nullptr;
+    char* device = nullptr;  // header, requests, chunks0, chunks1, flagged
+    char* host = nullptr;    // pinned staging for the descriptors
+    bool busy = false;
+    std::vector<std::shared_ptr<ServedRequest>> members;
+    WaveArgs args{};
+};
+
+}  // namespace gg
+
+struct gg_server {
+    gg_context* ctx = nullptr;
+    const gg_volume* vol = nullptr;
+    gg_server_config cfg{};
+    uint32_t max_requests = 1024;
+    uint32_t max_chunks = 0;
+    uint32_t flagged_capacity = 0;
+    uint64_t slot_bytes = 0;
+    int grid = 0;
+    cudaStream_t build = nullptr, copy = nullptr, plain = nullptr;
+    cudaEvent_t built = nullptr, origin = nullptr;
+    std::vector<gg::WaveSlot> slots;
+    std::mutex mu;
+    std::condition_variable cv_work, cv_done;
+    std::deque<std::shared_ptr<gg::ServedRequest>> pending;
+    std::vector<std::shared_ptr<gg::ServedRequest>> admitted;
+    std::map<uint64_t, std::shared_ptr<gg::ServedRequest>> all;
+    uint64_t next_ticket = 1;
+    uint64_t memory_used = 0;
+    bool stop = false;
+    int fatal = GG_OK;
+    std::string fatal_sentence;
+    std::thread worker;
+    uint64_t total_requests = 0, total_steps = 0, total_waves = 0;
+    std::vector<std::pair<double, double>> intervals;  // wave device intervals, seconds after `origin`
+    int next_slot = 0;
+};
+
+namespace gg {
+
+static uint64_t slot_offset_requests() { return sizeof(WaveHeader); }
+static uint64_t slot_offset_chunks0(const gg_server* s) { return slot_offset_requests() + (uint64_t)s->max_requests * sizeof(ServeRequest); }
+static uint64_t slot_offset_chunks1(const gg_server* s) { return slot_offset_chunks0(s) + (uint64_t)s->max_chunks * sizeof(ServeChunk); }
+static uint64_t slot_offset_flagged(const gg_server* s) { return slot_offset_chunks1(s) + (uint64_t)s->max_chunks * sizeof(ServeChunk); }
+
+static int capture_wave_graph(gg_server* s, WaveSlot& w) {
+    cudaGraph_t g = nullptr;
+    GG_CUDA(cudaStreamBeginCapture(w.stream, cudaStreamCaptureModeThreadLocal), "wave capture");
+    serve_kernel<<<s->grid, kServeThreads, 0, w.stream>>>(w.args);
+    serve_reintegrate_kernel<<<s->ctx->sm_count * 2, 128, 0, w.stream>>>(w.args);
+    cudaError_t e = cudaStreamEndCapture(w.stream, &g);
+    GG_CUDA(e, "wave capture");
+    e = cudaGraphInstantiate(&w.graph, g, 0);
+    cudaGraphDestroy(g);
+    GG_CUDA(e, "wave graph instantiate");
+    return GG_OK;
+}
+
+static int admit(gg_server* s, const std::shared_ptr<ServedRequest>& r) {
+    gg_context* ctx = s->ctx;
+    const uint64_t px = r->rays;
+    GG_CUDA(cudaMallocAsync((void**)&r->d_color, px * 8u, s->build), "request target");
+    if (r->q.debug_output) GG_CUDA(cudaMallocAsync((void**)&r->d_debug, px * 8u, s->build), "request debug target");
+    GG_CUDA(cudaMallocAsync((void**)&r->d_stats, 128, s->build), "request counters");
+    GG_CUDA(cudaMemsetAsync(r->d_stats, 0, 128, s->build), "request counters");
+    if (r->q.spin == 0.0f) {
+        GG_CUDA(cudaMallocAsync((void**)&r->sweep.camera, SWEEP_TABLE_SIZE * sizeof(float), s->build), "camera table");
+        GG_CUDA(cudaMallocAsync((void**)&r->sweep.sky, SWEEP_TABLE_SIZE * sizeof(float), s->build), "sky table");
+        GG_CHECK(sweep_build(ctx, s->build, (double)r->q.distance, &r->sweep));
+        sweep_apply(ctx, &r->sweep, &r->u);
+    }
+    r->result.admitted = now_seconds();
+    return GG_OK;
+}
+
+static void release(gg_server* s, ServedRequest& r) {
+    cudaFreeAsync(r.d_color, s->copy);
+    if (r.d_debug) cudaFreeAsync(r.d_debug, s->copy);
+    cudaFreeAsync(r.d_stats, s->copy);
+    r.d_color = nullptr;
+    r.d_debug = nullptr;
+    r.d_stats = nullptr;
+    if (r.sweep.camera) {
+        cudaFreeAsync(r.sweep.camera, s->copy);
+        cudaFreeAsync(r.sweep.sky, s->copy);
+        r.sweep.camera = r.sweep.sky = nullptr;
+    }
+}
+
+// Start the copy of a request whose rays are all done.
+static int start_copy(gg_server* s, ServedRequest& r, cudaEvent_t after) {
+    if (after) GG_CUDA(cudaStreamWaitEvent(s->copy, after, 0), "copy ordering");
+    const uint64_t px = r.rays;
+    GG_CUDA(cudaMemcpyAsync(r.q.output, r.d_color, px * 8u, cudaMemcpyDeviceToHost, s->copy), "request readback");
+    if (r.d_debug)
+        GG_CUDA(cudaMemcpyAsync(r.q.debug_output, r.d_debug, px * 8u, cudaMemcpyDeviceToHost, s->copy), "request readback");
+    GG_CUDA(cudaMemcpyAsync(r.host_stats, r.d_stats, 80, cudaMemcpyDeviceToHost, s->copy), "request counters");
+    GG_CUDA(cudaEventCreateWithFlags(&r.copied, cudaEventDisableTiming), "copy event");
+    GG_CUDA(cudaEventRecord(r.copied, s->copy), "copy event");
+    r.copying = true;
+    return GG_OK;
+}
+
+// Pack the next wave into slot w from the admitted requests, round-robin.
+static bool form_wave(gg_server* s, WaveSlot& w) {
+    std::vector<std::shared_ptr<ServedRequest>> cands;
+    for (auto& r : s->admitted)
+        if (r->next_ray < r->rays) cands.push_back(r);
+    if (cands.empty()) return false;
+    WaveHeader* hdr = reinterpret_cast<WaveHeader*>(w.host);
+    std::memset(hdr, 0, sizeof *hdr);
+    ServeRequest* reqs = reinterpret_cast<ServeRequest*>(w.host + slot_offset_requests());
+    ServeChunk* c0 = reinterpret_cast<ServeChunk*>(w.host + slot_offset_chunks0(s));
+    ServeChunk* c1 = reinterpret_cast<ServeChunk*>(w.host + slot_offset_chunks1(s));
+    const uint32_t chunk = s->cfg.chunk_rays;
+    uint64_t budget = s->cfg.wave_rays;
+    w.members.clear();
+    std::vector<uint32_t> local(cands.size(), UINT32_MAX);
+    bool progress = true;
+    while (budget > 0 && progress) {
+        progress = false;
+        const uint64_t share = std::max<uint64_t>(chunk, budget / cands.size());
+        for (size_t i = 0; i < cands.size() && budget > 0; ++i) {
+            ServedRequest& r = *cands[i];
+            if (r.next_ray >= r.rays) continue;
+            if (local[i] == UINT32_MAX) {
+                if (hdr->request_count >= s->max_requests) continue;
+                local[i] = hdr->request_count++;
+                ServeRequest& d = reqs[local[i]];
+                std::memset(&d, 0, sizeof d);
+                d.u = r.u;
+                d.camera_table = r.sweep.camera;
+                d.sky_table = r.sweep.sky;
+                d.color = r.d_color;
+                d.debug = r.d_debug;
+                d.stats = r.d_stats;
+                w.members.push_back(cands[i]);
+                r.waves_pending += 1;
+            }
+            const int kind = r.u.spin > 0.0f ? 1 : 0;
+            uint64_t take = std::min<uint64_t>({share, budget, (uint64_t)(r.rays - r.next_ray)});
+            while (take > 0 && hdr->chunk_count[kind] < s->max_chunks) {
+                uint32_t n = (uint32_t)std::min<uint64_t>(chunk, take);
+                ServeChunk& ch = (kind ? c1 : c0)[hdr->chunk_count[kind]++];
+                ch.request = local[i];
+                ch.first = r.next_ray;
+                ch.count = n;
+                ch.pad = 0;
+                r.next_ray += n;
+                take -= n;
+                budget -= n;
+                progress = true;
+            }
+        }
+    }
+    return hdr->request_count > 0;
+}
+
+static int launch_wave(gg_server* s, WaveSlot& w) {
+    WaveHeader* hdr = reinterpret_cast<WaveHeader*>(w.host);
+    GG_CUDA(cudaStreamWaitEvent(w.stream, s->built, 0), "wave ordering");
+    GG_CUDA(cudaMemcpyAsync(w.device, w.host, sizeof(WaveHeader) + hdr->request_count * sizeof(ServeRequest),
+                            cudaMemcpyHostToDevice, w.stream),
+            "wave upload");
+    if (hdr->chunk_count[0])
+        GG_CUDA(cudaMemcpyAsync(w.device + slot_offset_chunks0(s), w.host + slot_offset_chunks0(s),
+                                hdr->chunk_count[0] * sizeof(ServeChunk), cudaMemcpyHostToDevice, w.stream),
+                "wave upload");
+    if (hdr->chunk_count[1])
+        GG_CUDA(cudaMemcpyAsync(w.device + slot_offset_chunks1(s), w.host + slot_offset_chunks1(s),
+                                hdr->chunk_count[1] * sizeof(ServeChunk), cudaMemcpyHostToDevice, w.stream),
+                "wave upload");
+    GG_CUDA(cudaEventRecord(w.start, w.stream), "wave event");
+    GG_CUDA(cudaGraphLaunch(w.graph, w.stream), "wave launch");
+    GG_CUDA(cudaEventRecord(w.stop, w.stream), "wave event");
+    w.busy = true;
+    s->total_waves += 1;
+    return GG_OK;
+}
+
+static int finish_wave(gg_server* s, WaveSlot& w) {
+    float t0 = 0.0f, t1 = 0.0f;
+    GG_CUDA(cudaEventElapsedTime(&t0, s->origin, w.start), "wave timing");
+    GG_CUDA(cudaEventElapsedTime(&t1, s->origin, w.stop), "wave timing");
+    s->intervals.emplace_back((double)t0 * 1e-3, (double)t1 * 1e-3);
+    for (auto& r : w.members) {
+        r->waves_pending -= 1;
+        if (r->waves_pending == 0 && r->next_ray >= r->rays && !r->copying) GG_CHECK(start_copy(s, *r, w.stop));
+    }
+    w.members.clear();
+    w.busy = false;
+    return GG_OK;
+}
+
+// The per-request baseline: one request at a time, plain FP32 image kernel.
+static int run_plain(gg_server* s, ServedRequest& r) {
+    gg_context* ctx = s->ctx;
+    GG_CUDA(cudaStreamWaitEvent(s->plain, s->built, 0), "plain ordering");
+    MarchParams p = make_params(ctx, s->vol, r.u, r.q.spin == 0.0f ? &r.sweep : nullptr);
+    p.color = r.d_color;
+    p.debug = r.d_debug;
+    p.target_width = r.q.width;
+    p.target_height = r.q.height;
+    p.counters = reinterpret_cast<MarchCounters*>(r.d_stats + 8);
+    p.stats = r.d_stats;
+    GG_CUDA(cudaEventRecord(s->slots[0].start, s->plain), "plain event");
+    GG_CHECK(launch_plain_image(p, s->plain));
+    GG_CUDA(cudaEventRecord(s->slots[0].stop, s->plain), "plain event");
+    r.next_ray = r.rays;
+    s->total_waves += 1;
+    GG_CHECK(start_copy(s, r, s->slots[0].stop));
+    // Serial: the next request starts after this one's pixels are home.
+    GG_CUDA(cudaEventSynchronize(r.copied), "plain march");
+    float t0 = 0.0f, t1 = 0.0f;
+    GG_CUDA(cudaEventElapsedTime(&t0, s->origin, s->slots[0].start), "plain timing");
+    GG_CUDA(cudaEventElapsedTime(&t1, s->origin, s->slots[0].stop), "plain timing");
+    s->intervals.emplace_back((double)t0 * 1e-3, (double)t1 * 1e-3);
+    return GG_OK;
+}
+
+static void complete_request(gg_server* s, ServedRequest& r) {
+    r.result.finished = now_seconds();
+    r.result.ray_steps = r.host_stats[0];
+    r.result.samples = r.host_stats[1];
+    r.result.fp64_rays = r.host_stats[2];
+    if (s->cfg.mode == GG_SERVE_SERIAL_PLAIN) {
+        std::memcpy(&r.result.counters, &r.host_stats[8], sizeof(MarchCounters));
+    } else {
+        r.result.counters.rays = (uint32_t)r.host_stats[3];
+        r.result.counters.overDriftBudget = (uint32_t)r.host_stats[4];
+        r.result.counters.exhausted = (uint32_t)r.host_stats[5];
+        r.result.counters.captured = (uint32_t)r.host_stats[6];
+    }
+    r.result.status = GG_OK;
+    cudaEventDestroy(r.copied);
+    r.copied = nullptr;
+    release(s, r);
+    s->memory_used -= r.footprint;
+    s->total_requests += 1;
+    s->total_steps += r.result.ray_steps;
+    r.done = true;
+}
+
+static void worker_loop(gg_server* s) {
+    cudaSetDevice(s->ctx->device);
+    std::unique_lock<std::mutex> lock(s->mu);
+    // Runs for the server's lifetime: until destroy() asks it to stop and
+    // every submitted request has completed, or a device error.
+    for (bool running = true; running;) {
+        int status = GG_OK;
+        // Admission in arrival order while the footprint fits.
+        bool admitted_any = false;
+        while (!s->pending.empty() && s->memory_used + s->pending.front()->footprint <= s->cfg.memory_bytes &&
+               (s->cfg.mode != GG_SERVE_SERIAL_PLAIN || s->admitted.empty())) {
+            auto r = s->pending.front();
+            s->pending.pop_front();
+            s->memory_used += r->footprint;
+            status = admit(s, r);
+            if (status != GG_OK) break;
+            s->admitted.push_back(r);
+            admitted_any = true;
+        }
+        if (status == GG_OK && admitted_any) status = cuda_status(cudaEventRecord(s->built, s->build), "admission");
+        // Launch work.
+        if (status == GG_OK) {
+            if (s->cfg.mode == GG_SERVE_SERIAL_PLAIN) {
+                for (auto& r : s->admitted)
+                    if (r->next_ray < r->rays && status == GG_OK) {
+                        lock.unlock();
+                        status = run_plain(s, *r);
+                        lock.lock();
+                    }
+            } else {
+                for (uint32_t k = 0; k < s->slots.size() && status == GG_OK; ++k) {
+                    WaveSlot& w = s->slots[(s->next_slot + k) % s->slots.size()];
+                    if (w.busy) continue;
+                    if (!form_wave(s, w)) break;
+                    status = launch_wave(s, w);
+                    s->next_slot = (int)((&w - &s->slots[0]) + 1) % (int)s->slots.size();
+                }
+            }
+        }
+        // Retire finished waves and copies.
+        bool any_busy = false;
+        for (auto& w : s->slots) {
+            if (!w.busy || status != GG_OK) continue;
+            cudaError_t q = cudaEventQuery(w.stop);
+            if (q == cudaSuccess) status = finish_wave(s, w);
+            else if (q != cudaErrorNotReady) status = cuda_status(q, "wave");
+            else any_busy = true;
+        }
+        bool finished_any = false;
+        for (auto it = s->admitted.begin(); it != s->admitted.end() && status == GG_OK;) {
+            ServedRequest& r = **it;
+            if (r.copying) {
+                cudaError_t q = cudaEventQuery(r.copied);
+                if (q == cudaSuccess) {
+                    complete_request(s, r);
+                    finished_any = true;
+                    it = s->admitted.erase(it);
+                    continue;
+                }
+                if (q != cudaErrorNotReady) status = cuda_status(q, "request readback");
+            }
+            ++it;
+        }
+        if (status != GG_OK) {
+            s->fatal = status;
+            s->fatal_sentence = gg_last_error();
+            s->cv_done.notify_all();
+            return;
+        }
+        if (finished_any) s->cv_done.notify_all();
+        bool work_left = !s->pending.empty() || !s->admitted.empty() || any_busy;
+        if (s->stop && !work_left) {
+            running = false;
+        } else if (work_left) {
+            // Devices run asynchronously; poll at a short interval.
+            s->cv_work.wait_for(lock, std::chrono::microseconds(50));
+        } else {
+            s->cv_work.wait(lock, [s] { return s->stop || !s->pending.empty(); });
+        }
+    }
+}
+
+}  // namespace gg
+
+using namespace gg;
+
+extern "C" {
+
+GG_API int gg_server_create(gg_context* ctx, const gg_volume* vol, const gg_server_config* config, gg_server** out) {
+    if (!ctx || !out) return gg::fail(GG_ERR_INVALID_ARGUMENT, "gg_server_create needs a context and an output.");
+    *out = nullptr;
+    if (vol && vol->ctx != ctx) return gg::fail(GG_ERR_INVALID_ARGUMENT, "gg_server_create: volume from another context.");
+    std::lock_guard<std::recursive_mutex> clock(ctx->mu);
+    GG_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
+    std::unique_ptr<gg_server> s(new gg_server());
+    s->ctx = ctx;
+    s->vol = vol;
+    if (config) s->cfg = *config;
+    if (s->cfg.mode != GG_SERVE_BATCHED && s->cfg.mode != GG_SERVE_SERIAL_PLAIN)
+        return gg::fail(GG_ERR_INVALID_ARGUMENT, "Unknown serving mode %d.", s->cfg.mode);
+    if (s->cfg.memory_bytes == 0) s->cfg.memory_bytes = (ctx->budget - ctx->used) / 4;
+    if (ctx->used + s->cfg.memory_bytes > ctx->budget)
+        return gg::fail(GG_ERR_OVER_BUDGET, "The server asks for %llu bytes but the budget has %llu left.",
+                        (unsigned long long)s->cfg.memory_bytes, (unsigned long long)(ctx->budget - ctx->used));
+    if (s->cfg.wave_rays == 0) s->cfg.wave_rays = 4u << 20;
+    if (s->cfg.chunk_rays == 0) s->cfg.chunk_rays = 256;
+    if (s->cfg.max_waves_in_flight == 0) s->cfg.max_waves_in_flight = 2;
+    if (s->cfg.max_waves_in_flight > 4) s->cfg.max_waves_in_flight = 4;
+    if (s->cfg.chunk_rays < 32 || s->cfg.chunk_rays > 65536)
+        return gg::fail(GG_ERR_INVALID_ARGUMENT, "chunk_rays %u is outside 32..65536.", s->cfg.chunk_rays);
+    s->max_chunks = s->cfg.wave_rays / s->cfg.chunk_rays + 1024;
+    s->flagged_capacity = s->cfg.wave_rays / 8;
+    s->slot_bytes = gg::slot_offset_flagged(s.get()) + (uint64_t)s->flagged_capacity * 8u;
+    int blocks = 0;
+    GG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, gg::serve_kernel, gg::kServeThreads, 0), "occupancy");
+    s->grid = std::max(1, blocks) * ctx->sm_count;
+    GG_CUDA(cudaStreamCreateWithFlags(&s->build, cudaStreamNonBlocking), "server streams");
+    GG_CUDA(cudaStreamCreateWithFlags(&s->copy, cudaStreamNonBlocking), "server streams");
+    GG_CUDA(cudaStreamCreateWithFlags(&s->plain, cudaStreamNonBlocking), "server streams");
+    GG_CUDA(cudaEventCreateWithFlags(&s->built, cudaEventDisableTiming), "server events");
+    GG_CUDA(cudaEventCreate(&s->origin), "server events");
+    GG_CUDA(cudaEventRecord(s->built, s->build), "server events");
+    GG_CUDA(cudaEventRecord(s->origin, s->build), "server events");
+    const int nslots = s->cfg.mode == GG_SERVE_SERIAL_PLAIN ? 1 : (int)s->cfg.max_waves_in_flight;
+    s->slots.resize(nslots);
+    for (auto& w : s->slots) {
+        GG_CUDA(cudaStreamCreateWithFlags(&w.stream, cudaStreamNonBlocking), "wave stream");
+        GG_CUDA(cudaEventCreate(&w.start), "wave events");
+        GG_CUDA(cudaEventCreate(&w.stop), "wave events");
+        if (s->cfg.mode == GG_SERVE_SERIAL_PLAIN) continue;
+        GG_CHECK(gg::device_alloc(ctx, s->slot_bytes, (void**)&w.device, "wave descriptors"));
+        GG_CUDA(cudaHostAlloc((void**)&w.host, gg::slot_offset_flagged(s.get()), cudaHostAllocDefault), "wave staging");
+        w.args.header = reinterpret_cast<gg::WaveHeader*>(w.device);
+        w.args.requests = reinterpret_cast<const gg::ServeRequest*>(w.device + gg::slot_offset_requests());
+        w.args.chunks0 = reinterpret_cast<const gg::ServeChunk*>(w.device + gg::slot_offset_chunks0(s.get()));
+        w.args.chunks1 = reinterpret_cast<const gg::ServeChunk*>(w.device + gg::slot_offset_chunks1(s.get()));
+        w.args.flagged = reinterpret_cast<unsigned long long*>(w.device + gg::slot_offset_flagged(s.get()));
+        w.args.flagged_capacity = s->flagged_capacity;
+        w.args.sphere_table = ctx->sphere_table;
+        w.args.blackbody = ctx->blackbody;
+        w.args.emission = vol ? vol->emission_tex : 0;
+        w.args.velocity = vol ? vol->velocity_tex : 0;
+        GG_CHECK(gg::capture_wave_graph(s.get(), w));
+    }
+    GG_CUDA(cudaStreamSynchronize(s->build), "server set-up");
+    ctx->used += s->cfg.memory_bytes;  // reserved for admitted requests
+    s->worker = std::thread(gg::worker_loop, s.get());
+    *out = s.release();
+    return GG_OK;
+}
+
+GG_API void gg_server_destroy(gg_server* s) {
+    if (!s) return;
+    {
+        std::lock_guard<std::mutex> lock(s->mu);
+        s->stop = true;
+    }
+    s->cv_work.notify_all();
+    if (s->worker.joinable()) s->worker.join();
+    gg_context* ctx = s->ctx;
+    cudaSetDevice(ctx->device);
+    for (auto& w : s->slots) {
+        if (w.stream) cudaStreamSynchronize(w.stream);
+        if (w.graph) cudaGraphExecDestroy(w.graph);
+        if (w.device) gg::device_free(ctx, w.device, s->slot_bytes);
+        if (w.host) cudaFreeHost(w.host);
+        if (w.start) cudaEventDestroy(w.start);
+        if (w.stop) cudaEventDestroy(w.stop);
+        if (w.stream) cudaStreamDestroy(w.stream);
+    }
+    cudaStreamSynchronize(s->copy);
+    cudaStreamSynchronize(s->build);
+    for (auto& r : s->admitted) gg::release(s, *r);
+    cudaStreamSynchronize(s->copy);
+    ctx->used -= std::min(ctx->used, s->cfg.memory_bytes);
+    cudaEventDestroy(s->built);
+    cudaEventDestroy(s->origin);
+    cudaStreamDestroy(s->build);
+    cudaStreamDestroy(s->copy);
+    cudaStreamDestroy(s->plain);
+    delete s;
+}
+
+GG_API int gg_server_submit(gg_server* s, const gg_request* req, uint64_t* ticket) {
+    if (!s || !req || !ticket) return gg::fail(GG_ERR_INVALID_ARGUMENT, "gg_server_submit needs a server, a request and a ticket.");
+    if (req->width == 0 || req->height == 0 || req->width > 16384 || req->height > 16384 ||
+        (uint64_t)req->width * req->height > (1ull << 31))
+        return gg::fail(GG_ERR_INVALID_ARGUMENT, "Request size %ux%u is outside 1..16384.", req->width, req->height);
+    if (req->step_cap == 0 || req->step_cap > STEP_CAP_STILL)
+        return gg::fail(GG_ERR_INVALID_ARGUMENT, "Step cap %u is outside 1..%u.", req->step_cap, STEP_CAP_STILL);
+    if (!(req->spin >= 0.0f && req->spin < 1.0f))
+        return gg::fail(GG_ERR_INVALID_ARGUMENT, "Spin %g is outside [0, 1).", (double)req->spin);
+    if (!(req->distance > VOLUME_HALF_EXTENT) || !(req->distance < 1e4f))
+        return gg::fail(GG_ERR_INVALID_ARGUMENT, "Camera distance %g is outside (%g, 1e4).", (double)req->distance,
+                        (double)VOLUME_HALF_EXTENT);
+    if (!(req->fov_y > 0.0f && req->fov_y < 3.1f)) return gg::fail(GG_ERR_INVALID_ARGUMENT, "Field of view %g is invalid.", (double)req->fov_y);
+    if (!req->output) return gg::fail(GG_ERR_INVALID_ARGUMENT, "The request has no output buffer.");
+    auto r = std::make_shared<gg::ServedRequest>();
+    r->q = *req;
+    r->u = gg::request_uniforms(*req);
+    r->rays = req->width * req->height;
+    r->footprint = (uint64_t)r->rays * (req->debug_output ? 16u : 8u) + 128u + 2u * SWEEP_TABLE_SIZE * 4u;
+    std::lock_guard<std::mutex> lock(s->mu);
+    if (s->fatal != GG_OK) return gg::fail(s->fatal, "The server stopped after a device error: %s", s->fatal_sentence.c_str());
+    if (r->footprint > s->cfg.memory_bytes)
+        return gg::fail(GG_ERR_OVER_BUDGET, "A %ux%u request needs %llu bytes but the server has %llu.", req->width,
+                        req->height, (unsigned long long)r->footprint, (unsigned long long)s->cfg.memory_bytes);
+    r->ticket = s->next_ticket++;
+    r->result.submitted = gg::now_seconds();
+    s->pending.push_back(r);
+    s->all[r->ticket] = r;
+    *ticket = r->ticket;
+    s->cv_work.notify_one();
+    return GG_OK;
+}
+
+GG_API int gg_server_poll(gg_server* s, uint64_t ticket, int* done) {
+    if (!s || !done) return gg::fail(GG_ERR_INVALID_ARGUMENT, "gg_server_poll needs a server and an output.");
+    std::lock_guard<std::mutex> lock(s->mu);
+    auto it = s->all.find(ticket);
+    if (it == s->all.end()) return gg::fail(GG_ERR_INVALID_ARGUMENT, "Unknown ticket %llu.", (unsigned long long)ticket);
+    if (s->fatal != GG_OK) return gg::fail(s->fatal, "The server stopped after a device error: %s", s->fatal_sentence.c_str());
+    *done = it->second->done ? 1 : 0;
+    return GG_OK;
+}
+
+GG_API int gg_server_wait(gg_server* s, uint64_t ticket, double timeout_s, gg_request_result* result) {
+    if (!s) return gg::fail(GG_ERR_INVALID_ARGUMENT, "gg_server_wait needs a server.");
+    std::unique_lock<std::mutex> lock(s->mu);
+    auto it = s->all.find(ticket);
+    if (it == s->all.end()) return gg::fail(GG_ERR_INVALID_ARGUMENT, "Unknown ticket %llu.", (unsigned long long)ticket);
+    auto r = it->second;
+    bool ok = s->cv_done.wait_for(lock, std::chrono::duration<double>(timeout_s),
+                                  [&] { return r->done || s->fatal != GG_OK; });
+    if (s->fatal != GG_OK) return gg::fail(s->fatal, "The server stopped after a device error: %s", s->fatal_sentence.c_str());
+    if (!ok) return gg::fail(GG_ERR_TIMEOUT, "Request %llu is not done after %g s.", (unsigned long long)ticket, timeout_s);
+    if (result) *result = r->result;
+    s->all.erase(it);
+    return GG_OK;
+}
+
+GG_API int gg_server_totals(gg_server* s, int reset, uint64_t* requests, uint64_t* ray_steps, uint64_t* launches,
+                            double* busy_seconds, double* span_seconds) {
+    if (!s) return gg::fail(GG_ERR_INVALID_ARGUMENT, "gg_server_totals needs a server.");
+    std::lock_guard<std::mutex> lock(s->mu);
+    if (requests) *requests = s->total_requests;
+    if (ray_steps) *ray_steps = s->total_steps;
+    if (launches) *launches = s->total_waves;
+    // Union of the launch intervals: waves on different streams overlap.
+    std::vector<std::pair<double, double>> iv = s->intervals;
+    std::sort(iv.begin(), iv.end());
+    double busy = 0.0, end = -1e300, first = 1e300, last = -1e300;
+    for (auto& p : iv) {
+        double a = std::max(p.first, end);
+        if (p.second > a) busy += p.second - a;
+        end = std::max(end, p.second);
+        first = std::min(first, p.first);
+        last = std::max(last, p.second);
+    }
+    if (busy_seconds) *busy_seconds = busy;
+    if (span_seconds) *span_seconds = iv.empty() ? 0.0 : last - first;
+    if (reset) {
+        s->total_requests = s->total_steps = s->total_waves = 0;
+        s->intervals.clear();
+    }
+    return GG_OK;
+}
+
+}  // extern "C"

@@ -109,6 +109,7 @@ int sweep_build(gg_context* ctx, cudaStream_t stream, double camera_radius, gg_s
     if (!(camera_radius > VOLUME_HALF_EXTENT))
         return fail(GG_ERR_INVALID_ARGUMENT, "The sweep tables need a camera outside the r = %.0f sphere, not r = %g.",
                     (double)VOLUME_HALF_EXTENT, camera_radius);
+    // Callers may supply stream-ordered buffers; otherwise they come from the budget.
     if (!out->camera) GG_CHECK(device_alloc(ctx, SWEEP_TABLE_SIZE * sizeof(float), (void**)&out->camera, "camera sweep table"));
     if (!out->sky) GG_CHECK(device_alloc(ctx, SWEEP_TABLE_SIZE * sizeof(float), (void**)&out->sky, "sky sweep table"));
     const double entry = (double)VOLUME_HALF_EXTENT - 1.0;

@@ -235,6 +235,11 @@ class Context:
         check(lib().gg_tables_read(self.handle, ptr(s), ptr(c), ptr(k)))
         return s, c, k
 
+    def fp32_peak_tflops(self) -> float:
+        t = C.c_double()
+        check(lib().gg_measure_fp32_peak(self.handle, C.byref(t)))
+        return t.value
+
     def blackbody(self) -> np.ndarray:
         out = np.zeros((256, 4), np.float32)
         check(lib().gg_context_blackbody(self.handle, out.ctypes.data_as(L.f32p), 256))
@@ -510,3 +515,79 @@ def write_png(path: str, rgba8: np.ndarray):
     rgba8 = np.ascontiguousarray(rgba8, np.uint8)
     h, w = rgba8.shape[:2]
     check(lib().gg_write_png(path.encode(), ptr(rgba8), w, h))
+
+
+@dataclass
+class RequestSpec:
+    """One still request (gg_request): orbit camera, size, step budget, spin."""
+
+    width: int
+    height: int
+    step_cap: int = 4096
+    spin: float = 0.0
+    azimuth: float = 0.6
+    elevation: float = 0.32
+    distance: float = 52.0
+    fov_y: float = 50.0 * math.pi / 180.0
+    star_seed: int = 1
+    flags: int = 0
+
+
+class Server:
+    """gg_server: continuous batching (SERVE_BATCHED) or the serial plain
+    per-request baseline (SERVE_SERIAL_PLAIN) over one resident volume."""
+
+    def __init__(self, ctx: Context, vol: Volume | None, mode: int = T.SERVE_BATCHED, memory_bytes: int = 0,
+                 wave_rays: int = 0, chunk_rays: int = 0, max_waves_in_flight: int = 0):
+        self.ctx = ctx
+        self.handle = C.c_void_p()
+        cfg = T.ServerConfig(mode, memory_bytes, wave_rays, chunk_rays, max_waves_in_flight)
+        check(lib().gg_server_create(ctx.handle, vol.handle if vol else None, C.byref(cfg), C.byref(self.handle)))
+        ctx.adopt(self)
+        self._buffers = {}
+
+    def close(self):
+        if self.handle:
+            lib().gg_server_destroy(self.handle)
+            self.handle = C.c_void_p()
+            self._buffers.clear()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def submit(self, spec: RequestSpec, output: np.ndarray | None = None, debug: bool = False) -> int:
+        """Queue a request; `output` (height*width*4 float16, kept alive here)
+        receives the pixels."""
+        n = spec.width * spec.height
+        if output is None:
+            output = np.zeros((n, 4), np.float16)
+        dbg = np.zeros((n, 4), np.float16) if debug else None
+        q = T.Request(spec.azimuth, spec.elevation, spec.distance, spec.fov_y, spec.width, spec.height,
+                      spec.step_cap, spec.spin, spec.star_seed & 0xFFFFFFFF, spec.flags,
+                      output.ctypes.data, dbg.ctypes.data if dbg is not None else None)
+        t = C.c_uint64()
+        check(lib().gg_server_submit(self.handle, C.byref(q), C.byref(t)))
+        self._buffers[t.value] = (output, dbg)
+        return t.value
+
+    def poll(self, ticket: int) -> bool:
+        d = C.c_int()
+        check(lib().gg_server_poll(self.handle, ticket, C.byref(d)))
+        return bool(d.value)
+
+    def wait(self, ticket: int, timeout_s: float = 600.0):
+        """(pixels, debug-or-None, RequestResult)."""
+        res = T.RequestResult()
+        check(lib().gg_server_wait(self.handle, ticket, timeout_s, C.byref(res)))
+        out, dbg = self._buffers.pop(ticket)
+        return out, dbg, res
+
+    def totals(self, reset: bool = False):
+        a, b, c, d, e = C.c_uint64(), C.c_uint64(), C.c_uint64(), C.c_double(), C.c_double()
+        check(lib().gg_server_totals(self.handle, 1 if reset else 0, C.byref(a), C.byref(b), C.byref(c), C.byref(d),
+                                     C.byref(e)))
+        return {"requests": a.value, "ray_steps": b.value, "launches": c.value, "busy_seconds": d.value,
+                "span_seconds": e.value}

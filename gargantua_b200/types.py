@@ -133,6 +133,33 @@ class MarchCounters(C.Structure):
     _fields_ = [("rays", u32), ("overDriftBudget", u32), ("exhausted", u32), ("captured", u32)]
 
 
+class Request(C.Structure):
+    """gg_request (include/gargantua.h)."""
+
+    _fields_ = [
+        ("azimuth", f32), ("elevation", f32), ("distance", f32), ("fov_y", f32),
+        ("width", u32), ("height", u32), ("step_cap", u32), ("spin", f32), ("star_seed", u32), ("flags", u32),
+        ("output", C.c_void_p), ("debug_output", C.c_void_p),
+    ]
+
+
+class RequestResult(C.Structure):
+    _fields_ = [
+        ("submitted", C.c_double), ("admitted", C.c_double), ("finished", C.c_double),
+        ("ray_steps", C.c_uint64), ("samples", C.c_uint64), ("fp64_rays", C.c_uint64),
+        ("counters", MarchCounters), ("status", C.c_int),
+    ]
+
+
+class ServerConfig(C.Structure):
+    _fields_ = [("mode", C.c_int), ("memory_bytes", C.c_uint64), ("wave_rays", u32), ("chunk_rays", u32),
+                ("max_waves_in_flight", u32)]
+
+
+SERVE_BATCHED, SERVE_SERIAL_PLAIN = 0, 1
+REQUEST_NO_STARS, REQUEST_NO_REDSHIFT = 1, 2
+
+
 # Sizes the C header pins with static assertions (gargantua_types.h).
 LAYOUT = {
     Particle: 32,

@@ -257,6 +257,91 @@ GG_API int gg_tonemap(gg_targets* t, const PresentUniforms* u, uint8_t* rgba8);
  * Replaces Capture.writePNG (App/Capture.swift:80-94). */
 GG_API int gg_write_png(const char* path, const uint8_t* rgba8, uint32_t width, uint32_t height);
 
+/* ---------------------------------------------------------------- serving */
+
+/* One still request: an orbit camera (Camera.swift:15-33: azimuth,
+ * elevation, distance, vertical field of view in radians), an image size, a
+ * step budget (256 selects the interactive policy, anything above the still
+ * policy, Schwarzschild.swift:167-172), a spin (0 renders Schwarzschild with
+ * the sphere jump, > 0 Kerr) and a star seed. The server writes width*height
+ * rgba16f pixels into `output` (host memory the caller keeps alive until the
+ * request completes) and, when debug_output is not NULL, the debug target
+ * (drift, steps, outcome, 1). Kerr cameras beyond R_ESCAPE escape at
+ * camera distance + 10 instead of R_ESCAPE, so rays start inside the scene.
+ * Replaces a `--still` render (Still.swift:9-99) as a served unit of work. */
+typedef struct {
+    float azimuth, elevation, distance, fov_y;
+    uint32_t width, height;
+    uint32_t step_cap;
+    float spin;
+    uint32_t star_seed;
+    uint32_t flags; /* GG_REQUEST_* */
+    uint16_t* output;
+    uint16_t* debug_output;
+} gg_request;
+
+#define GG_REQUEST_NO_STARS 1u   /* starBrightness 0 */
+#define GG_REQUEST_NO_REDSHIFT 2u
+
+/* Per-request outcome, times in seconds on the server's monotonic clock. */
+typedef struct {
+    double submitted, admitted, finished;
+    uint64_t ray_steps, samples, fp64_rays;
+    MarchCounters counters;
+    int status;
+} gg_request_result;
+
+typedef enum {
+    /* Continuous batching: requests are admitted as device memory frees up,
+     * their rays packed across requests into persistent, work-stealing
+     * launches replayed from CUDA graphs, compensated FP32 with FP64
+     * re-integration of flagged rays. */
+    GG_SERVE_BATCHED = 0,
+    /* One request at a time through the plain FP32 image kernel
+     * (gg_march with GG_PRECISION_PLAIN), the per-request baseline. */
+    GG_SERVE_SERIAL_PLAIN = 1
+} gg_serve_mode;
+
+typedef struct {
+    int mode;                  /* gg_serve_mode */
+    uint64_t memory_bytes;     /* device memory for admitted requests' targets; 0: a quarter of the budget left */
+    uint32_t wave_rays;        /* rays packed into one persistent launch; 0: 4 Mi */
+    uint32_t chunk_rays;       /* rays per work-stealing chunk; 0: 256 */
+    uint32_t max_waves_in_flight; /* 0: 2 */
+} gg_server_config;
+
+/* A server over a resident volume (vol may be NULL: no gas). */
+GG_API int gg_server_create(gg_context* ctx, const gg_volume* vol, const gg_server_config* config, gg_server** out);
+
+/* Stop accepting work, finish what was submitted, release everything. */
+GG_API void gg_server_destroy(gg_server* s);
+
+/* Queue a request; *ticket identifies it. Returns GG_ERR_OVER_BUDGET when
+ * the request alone can never fit the server's memory. */
+GG_API int gg_server_submit(gg_server* s, const gg_request* req, uint64_t* ticket);
+
+/* *done = 1 once the request's pixels are in its host buffers. */
+GG_API int gg_server_poll(gg_server* s, uint64_t ticket, int* done);
+
+/* Block until the request completes or timeout_s passes (GG_ERR_TIMEOUT);
+ * on success fills *result (may be NULL) and forgets the ticket. */
+GG_API int gg_server_wait(gg_server* s, uint64_t ticket, double timeout_s, gg_request_result* result);
+
+/* Totals since creation or the last reset: requests completed, ray steps,
+ * launches (waves, or per-request kernels in the plain mode), device-busy
+ * seconds (union of the launches' CUDA-event intervals) and device span
+ * seconds (first launch start to last launch end, on the device clock).
+ * reset != 0 zeroes them after reading. Any output pointer may be NULL. */
+GG_API int gg_server_totals(gg_server* s, int reset, uint64_t* requests, uint64_t* ray_steps, uint64_t* launches,
+                            double* busy_seconds, double* span_seconds);
+
+/* ------------------------------------------------------------ measurement */
+
+/* FP32 throughput of this device measured with a dependent-FMA kernel over
+ * every SM (each FMA counted as two flops): the peak the march's roofline is
+ * quoted against. */
+GG_API int gg_measure_fp32_peak(gg_context* ctx, double* tflops);
+
 #ifdef __cplusplus
 }
 #endif

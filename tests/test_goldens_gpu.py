@@ -255,3 +255,98 @@ def test_shadow_kerr(world):
     retro = O.lib().o_kerr_bisect_critical_xi(spin, radius, -1.0, C.byref(st), iterations)
     measured = gpu_asym / abs(retro / pro)
     assert golden_passes(golden, measured), f"gpu {gpu_asym:.4f} vs oracle {abs(retro / pro):.4f}"
+
+
+# The same geodesic goldens through the compensated FP32 arithmetic the served
+# kernel runs (gg_probe with GG_PRECISION_COMPENSATED shares its lane code).
+
+COMP = 1
+
+
+def test_conservation_still_compensated(world):
+    import gargantua_b200 as g
+
+    golden = load_golden("conservation_still")
+    launches = g.camera_grid(g.OrbitCamera(), 16, 16, 960 / 540)
+    res = world["ctx"].probe(launches, probe_uniforms(g, world["ctx"], g.Settings.still()), COMP)
+    worst = float(res["drift"].max())
+    assert golden_passes(golden, worst), f"max drift {worst:.2e}"
+
+
+def test_parity_compensated(world):
+    import gargantua_b200 as g
+
+    golden = load_golden("parity")
+    launches = [g.as_float32_launch(l) for l in g.camera_grid(g.OrbitCamera(), 8, 8, 960 / 540)]
+    gpu = world["ctx"].probe(launches, probe_uniforms(g, world["ctx"], g.Settings.still()), COMP)
+    probes = np.array([np.concatenate([l.origin, l.direction]) for l in launches])
+    ref = O.integrate_batch(probes, O.still(), THREADS)
+    dist = np.linalg.norm(ref[:, :3] - gpu["position"].astype(np.float64), axis=1) / np.maximum(
+        np.linalg.norm(ref[:, :3], axis=1), 1.0)
+    mismatches = int((ref[:, 7].astype(int) != gpu["outcome"].astype(int)).sum())
+    assert golden_passes(golden, float(dist.max())) and mismatches == 0, (float(dist.max()), mismatches)
+
+
+def test_sky_compensated(world):
+    import gargantua_b200 as g
+
+    golden = load_golden("sky")
+    launches = [g.as_float32_launch(l) for l in g.camera_grid(g.OrbitCamera(), 8, 8, 960 / 540)]
+    gpu = world["ctx"].probe(launches, probe_uniforms(g, world["ctx"], g.Settings.still(), jump=True), COMP)
+    st = O.Settings(0.01, 0.02, 20.0, 2.02, 1e6, 400_000, 0.02, 20.0)
+    probes = np.array([np.concatenate([l.origin, l.direction]) for l in launches])
+    ref = O.integrate_batch(probes, st, THREADS)
+    worst, mism = 0.0, 0
+    for k in range(len(launches)):
+        ge, oe = gpu["outcome"][k] == 1, int(ref[k, 7]) == O.ESCAPED
+        if ge != oe:
+            mism += 1
+        elif ge:
+            worst = max(worst, math.acos(float(np.clip(ref[k, 3:6] @ gpu["direction"][k].astype(np.float64), -1, 1))))
+    assert golden_passes(golden, worst) and mism == 0, (worst, mism)
+
+
+def test_shadow_kerr_compensated(world):
+    import ctypes as C
+
+    import gargantua_b200 as g
+
+    golden = load_golden("shadow_kerr")
+    spin, radius, iterations = 0.9, 52.0, 40
+    u = probe_uniforms(g, world["ctx"], g.Settings.still(), spin=spin)
+
+    def xi(side):
+        low, high = 0.0, 12.0 / radius
+        for _ in range(iterations):
+            aim = 0.5 * (low + high)
+            res = world["ctx"].probe([g.Launch(np.array([radius, 0.0, 0.0]), np.array([-1.0, side * aim, 0.0]))], u,
+                                     COMP)
+            low, high = (aim, high) if res["outcome"][0] == 0 else (low, aim)
+        s = np.zeros(7)
+        O.lib().o_kerr_launch(spin, np.array([radius, 0.0, 0.0]), np.array([-1.0, side * 0.5 * (low + high), 0.0]), s)
+        return s[6] / s[5]
+
+    st = O.kerr_settings(4096)
+    pro = O.lib().o_kerr_bisect_critical_xi(spin, radius, 1.0, C.byref(st), iterations)
+    retro = O.lib().o_kerr_bisect_critical_xi(spin, radius, -1.0, C.byref(st), iterations)
+    measured = abs(xi(-1.0) / xi(1.0)) / abs(retro / pro)
+    assert golden_passes(golden, measured), measured
+
+
+def test_kerr_probe_parity_against_fp64_oracle(world):
+    """Kerr endpoints (plain and compensated) against the FP64 Kerr oracle
+    from identical float launches (the parity bar, 1e-3 of max(r, 1))."""
+    import gargantua_b200 as g
+
+    cam = g.OrbitCamera(0.3, 0.5, 50.0)
+    launches = [g.as_float32_launch(l) for l in g.camera_grid(cam, 8, 8, 16 / 9)]
+    probes = np.array([np.concatenate([l.origin, l.direction]) for l in launches])
+    ref = O.kerr_integrate_batch(0.9, probes, O.kerr_settings(4096), THREADS)
+    for prec in (0, COMP):
+        gpu = world["ctx"].probe(launches, probe_uniforms(g, world["ctx"], g.Settings.still(), spin=0.9), prec)
+        same = ref[:, 7].astype(int) == gpu["outcome"].astype(int)
+        assert same.mean() >= 0.95, same.mean()
+        esc = same & (ref[:, 7] == 1)
+        d = np.linalg.norm(ref[esc, :3] - gpu["position"][esc].astype(np.float64), axis=1) / np.maximum(
+            np.linalg.norm(ref[esc, :3], axis=1), 1.0)
+        assert d.max() < 1e-3, (prec, float(d.max()))
