@@ -1,19 +1,25 @@
-// The compensated FP32 march as a per-lane state machine: init from a camera
+// The compensated march as a per-lane state machine: init from a camera
 // ray, advance one RK4 step at a time, finish with the starfield. The served
-// persistent kernel refills lanes between steps; the compensated image and
-// probe kernels run one lane to completion. Both therefore execute exactly
-// the same arithmetic, which the goldens check through gg_probe.
+// persistent kernels refill lanes between steps; the compensated image and
+// probe kernels run one lane to completion; the FP64 re-integration runs the
+// same code in double. All therefore execute the same algorithm, and the
+// goldens check the FP32 instantiation through gg_probe.
 //
-// Arithmetic, against the reference's march (march.metal:51-184):
+// Against the reference's march (march.metal:51-184):
 //  - the same RK4 steps, step policy, capture/escape/sphere-exit logic and
 //    gather, so ray-step counts are the reference's;
-//  - each state += increment is TwoSum-compensated (march.cuh comp_add);
+//  - in FP32 each state += increment is TwoSum-compensated (comp_add);
 //  - one reciprocal per Schwarzschild derivative instead of four divides,
-//    using vDotDot = r phiDot^2 - vDot^2/r^2 appearing inside rDotDot;
-//    the Kerr derivative uses four reciprocals instead of eleven divides;
-//  - sin and cos from a Cody-Waite reduction by pi/2 and the Taylor series
-//    through r^9 / r^10 on |r| <= pi/4 (relative error below 2e-9 before
-//    float rounding) instead of the library's slow-path-capable sincosf;
+//    using vDotDot = r phiDot^2 - vDot^2/r^2 appearing inside rDotDot; the
+//    Kerr derivative uses three reciprocals instead of eleven divides;
+//  - the four RK4 stages run as a loop over one copy of the derivative,
+//    which keeps a step's instructions inside the SM's instruction cache;
+//  - sin and cos from a Cody-Waite reduction by pi/2 and Taylor series on
+//    |r| <= pi/4 (through r^9 / r^10 in FP32, r^17 / r^18 in FP64), and
+//    reciprocals from rcp.approx (FP32: within one ulp; FP64: refined by
+//    two Newton steps to full precision), instead of library calls with slow
+//    paths; the sine and cosine of the polar angle at the start of a Kerr
+//    step are carried over from the end of the previous one;
 //  - the Eddington-Finkelstein time v, which nothing downstream reads, is
 //    not integrated.
 #pragma once
@@ -21,6 +27,8 @@
 #include "march.cuh"
 
 namespace gg {
+
+// ----------------------------------------------------------------- math
 
 // sin and cos of a float angle of moderate size (|x| < 1e5).
 __device__ __forceinline__ void fast_sincos(float x, float* s_out, float* c_out) {
@@ -33,14 +41,14 @@ __device__ __forceinline__ void fast_sincos(float x, float* s_out, float* c_out)
     r = fmaf(-k, pio2_lo, r);
     float r2 = r * r;
     // sin r = r + r^3 (-1/3! + r^2 (1/5! + r^2 (-1/7! + r^2 / 9!)))
-    float ps = fmaf(r2, 2.75573192239859e-06f, -1.98412698412698e-04f);
-    ps = fmaf(r2, ps, 8.33333333333333e-03f);
-    ps = fmaf(r2, ps, -1.66666666666667e-01f);
+    float ps = fmaf(r2, (float)(1.0 / 362880.0), (float)(-1.0 / 5040.0));
+    ps = fmaf(r2, ps, (float)(1.0 / 120.0));
+    ps = fmaf(r2, ps, (float)(-1.0 / 6.0));
     float sr = fmaf(r * r2, ps, r);
     // cos r = 1 + r^2 (-1/2 + r^2 (1/4! + r^2 (-1/6! + r^2 (1/8! - r^2/10!))))
-    float pc = fmaf(r2, -2.75573192239859e-07f, 2.48015873015873e-05f);
-    pc = fmaf(r2, pc, -1.38888888888889e-03f);
-    pc = fmaf(r2, pc, 4.16666666666667e-02f);
+    float pc = fmaf(r2, (float)(-1.0 / 3628800.0), (float)(1.0 / 40320.0));
+    pc = fmaf(r2, pc, (float)(-1.0 / 720.0));
+    pc = fmaf(r2, pc, (float)(1.0 / 24.0));
     pc = fmaf(r2, pc, -0.5f);
     float cr = fmaf(r2, pc, 1.0f);
     int q = (int)k;
@@ -52,196 +60,259 @@ __device__ __forceinline__ void fast_sincos(float x, float* s_out, float* c_out)
     *c_out = c;
 }
 
-// Reciprocal to within one ulp (PTX rcp.approx: max error 1 ulp).
+// sin and cos of a double angle of moderate size: the same reduction with
+// pi/2 in three parts and the series through r^17 and r^18.
+__device__ __forceinline__ void fast_sincos(double x, double* s_out, double* c_out) {
+    const double two_over_pi = 6.36619772367581382433e-01;
+    const double pio2_hi = 1.57079601287841796875e+00;
+    const double pio2_mid = 3.13916478650481311129e-07;
+    const double pio2_lo = 1.05629990669874276403e-23;
+    double k = rint(x * two_over_pi);
+    double r = fma(-k, pio2_hi, x);
+    r = fma(-k, pio2_mid, r);
+    r = fma(-k, pio2_lo, r);
+    double r2 = r * r;
+    double ps = fma(r2, 1.0 / 355687428096000.0, -1.0 / 1307674368000.0);
+    ps = fma(r2, ps, 1.0 / 6227020800.0);
+    ps = fma(r2, ps, -1.0 / 39916800.0);
+    ps = fma(r2, ps, 1.0 / 362880.0);
+    ps = fma(r2, ps, -1.0 / 5040.0);
+    ps = fma(r2, ps, 1.0 / 120.0);
+    ps = fma(r2, ps, -1.0 / 6.0);
+    double sr = fma(r * r2, ps, r);
+    double pc = fma(r2, 1.0 / 6402373705728000.0, -1.0 / 20922789888000.0);
+    pc = fma(r2, pc, 1.0 / 87178291200.0);
+    pc = fma(r2, pc, -1.0 / 479001600.0);
+    pc = fma(r2, pc, 1.0 / 3628800.0);
+    pc = fma(r2, pc, -1.0 / 40320.0);
+    pc = fma(r2, pc, 1.0 / 720.0);
+    pc = fma(r2, pc, -1.0 / 24.0);
+    pc = fma(r2, pc, 0.5);
+    double cr = fma(-r2, pc, 1.0);
+    long long q = (long long)k;
+    double s = (q & 1) ? cr : sr;
+    double c = (q & 1) ? sr : cr;
+    if (q & 2) s = -s;
+    if ((q + 1) & 2) c = -c;
+    *s_out = s;
+    *c_out = c;
+}
+
+// Reciprocal: FP32 within one ulp (PTX rcp.approx); FP64 from the
+// approximate reciprocal refined by two Newton steps y += y (1 - x y).
 __device__ __forceinline__ float rcp(float x) {
     float y;
     asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
     return y;
 }
 
+__device__ __forceinline__ double rcp(double x) {
+    double y;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+    double e = fma(-x, y, 1.0);
+    y = fma(y, e, y);
+    e = fma(-x, y, 1.0);
+    return fma(y, e, y);
+}
+
+__device__ __forceinline__ float fmaT(float a, float b, float c) { return fmaf(a, b, c); }
+__device__ __forceinline__ double fmaT(double a, double b, double c) { return fma(a, b, c); }
+__device__ __forceinline__ float rsqrtT(float x) { return rsqrtf(x); }
+__device__ __forceinline__ double rsqrtT(double x) { return rcp(sqrt(x)); }
+
+// x += y; in FP32 the rounding error is carried in e (TwoSum, march.cuh).
+__device__ __forceinline__ void comp_addT(float& x, float& e, float y) { comp_add(x, e, y); }
+__device__ __forceinline__ void comp_addT(double& x, double& e, double y) { x += y; }
+
+template <typename R> __device__ __forceinline__ V3<R> v3_of(float3 a) { return v3<R>(R(a.x), R(a.y), R(a.z)); }
+
 // ------------------------------------------------------------ Schwarzschild
 
-struct SState {
-    float r, phi, vd, rd, pd;
+template <typename R> struct SState {
+    R r, phi, vd, rd, pd;
 };
 
 // Geodesic equations (Geodesic.h:42-49) with one reciprocal.
-__device__ __forceinline__ SState s_derivative(const SState& s) {
-    float inv_r = rcp(s.r);
-    float inv_r2 = inv_r * inv_r;
-    float vdd = s.r * (s.pd * s.pd) - (s.vd * s.vd) * inv_r2;
-    float f = fmaf(-2.0f, inv_r, 1.0f);
-    float rdd = fmaf(f, vdd, 2.0f * (s.rd * s.vd) * inv_r2);
-    float pdd = -2.0f * (s.rd * s.pd) * inv_r;
-    return SState{s.rd, s.pd, vdd, rdd, pdd};
+template <typename R> __device__ __forceinline__ SState<R> s_derivative(const SState<R>& s) {
+    R inv_r = rcp(s.r);
+    R inv_r2 = inv_r * inv_r;
+    R vdd = s.r * (s.pd * s.pd) - (s.vd * s.vd) * inv_r2;
+    R f = fmaT(R(-2), inv_r, R(1));
+    R rdd = fmaT(f, vdd, R(2) * (s.rd * s.vd) * inv_r2);
+    R pdd = R(-2) * (s.rd * s.pd) * inv_r;
+    return SState<R>{s.rd, s.pd, vdd, rdd, pdd};
 }
 
-__device__ __forceinline__ SState s_offset(const SState& s, const SState& k, float w) {
-    return SState{fmaf(k.r, w, s.r), fmaf(k.phi, w, s.phi), fmaf(k.vd, w, s.vd), fmaf(k.rd, w, s.rd), fmaf(k.pd, w, s.pd)};
+template <typename R> __device__ __forceinline__ SState<R> s_offset(const SState<R>& s, const SState<R>& k, R w) {
+    return SState<R>{fmaT(k.r, w, s.r), fmaT(k.phi, w, s.phi), fmaT(k.vd, w, s.vd), fmaT(k.rd, w, s.rd),
+                     fmaT(k.pd, w, s.pd)};
 }
 
 // The RK4 increment (k1 + 2 k2 + 2 k3 + k4) h / 6 (Geodesic.h:52-59).
-__device__ __forceinline__ SState s_increment(const SState& s, float h) {
-    const float hh = 0.5f * h;
-    SState k1 = s_derivative(s);
-    SState k2 = s_derivative(s_offset(s, k1, hh));
-    SState k3 = s_derivative(s_offset(s, k2, hh));
-    SState k4 = s_derivative(s_offset(s, k3, h));
-    const float w = h * (1.0f / 6.0f);
-    SState inc;
-    inc.r = (k1.r + 2.0f * k2.r + (2.0f * k3.r + k4.r)) * w;
-    inc.phi = (k1.phi + 2.0f * k2.phi + (2.0f * k3.phi + k4.phi)) * w;
-    inc.vd = (k1.vd + 2.0f * k2.vd + (2.0f * k3.vd + k4.vd)) * w;
-    inc.rd = (k1.rd + 2.0f * k2.rd + (2.0f * k3.rd + k4.rd)) * w;
-    inc.pd = (k1.pd + 2.0f * k2.pd + (2.0f * k3.pd + k4.pd)) * w;
-    return inc;
+template <typename R> __device__ __forceinline__ SState<R> s_increment(const SState<R>& s, R h) {
+    SState<R> acc{R(0), R(0), R(0), R(0), R(0)};
+    SState<R> x = s;
+#pragma unroll 1
+    for (int stage = 0; stage < 4; ++stage) {
+        SState<R> k = s_derivative(x);
+        R wk = (stage == 0 || stage == 3) ? R(1) : R(2);
+        acc = s_offset(acc, k, wk);
+        x = s_offset(s, k, stage < 2 ? R(0.5) * h : h);
+    }
+    const R w = h * (R(1) / R(6));
+    return SState<R>{acc.r * w, acc.phi * w, acc.vd * w, acc.rd * w, acc.pd * w};
 }
 
-struct SLane {
-    SState s, c;  // value and TwoSum error word
-    float3 e1, e2;
-    float energy, angular_momentum;  // launch values (the reference's ray.energy, ray.angularMomentum)
-    float e0, l0;                    // launch values of the integrated state, evaluated in double
+template <typename R> struct SLane {
+    SState<R> s, c;  // value and TwoSum error word (FP32)
+    V3<R> e1, e2;
+    R energy, angular_momentum;  // launch values (the reference's ray.energy, ray.angularMomentum)
+    double e0, l0;               // E and L of the state integration starts from, in double
     float3 color;
     float transmittance, travelled, weighted_depth, depth_weight;
-    float3 previous;
+    V3<R> previous;
     uint32_t steps, samples, outcome;
     float min_r;
     bool left_sphere;
 };
 
-__device__ __forceinline__ float3 s_position(const SLane& l, float* sn, float* cs) {
+template <typename R> __device__ __forceinline__ V3<R> s_position(const SLane<R>& l, R* sn, R* cs) {
     fast_sincos(l.s.phi, sn, cs);
-    return make_float3(l.s.r * fmaf(*cs, l.e1.x, *sn * l.e2.x), l.s.r * fmaf(*cs, l.e1.y, *sn * l.e2.y),
-                       l.s.r * fmaf(*cs, l.e1.z, *sn * l.e2.z));
+    return v3<R>(l.s.r * fmaT(*cs, l.e1.x, *sn * l.e2.x), l.s.r * fmaT(*cs, l.e1.y, *sn * l.e2.y),
+                 l.s.r * fmaT(*cs, l.e1.z, *sn * l.e2.z));
 }
 
 // Static-observer direction at the ray's radius (Geodesic.h:94-100).
-__device__ __forceinline__ float3 s_direction(const SLane& l, float sn, float cs) {
-    float3 radial = make_float3(fmaf(cs, l.e1.x, sn * l.e2.x), fmaf(cs, l.e1.y, sn * l.e2.y), fmaf(cs, l.e1.z, sn * l.e2.z));
-    float3 tang = make_float3(fmaf(-sn, l.e1.x, cs * l.e2.x), fmaf(-sn, l.e1.y, cs * l.e2.y), fmaf(-sn, l.e1.z, cs * l.e2.z));
-    float a = l.s.rd * rsqrtf(fmaxf(1.0f - 2.0f * rcp(l.s.r), 1e-6f));
-    float b = l.s.r * l.s.pd;
-    float3 local = make_float3(fmaf(a, radial.x, b * tang.x), fmaf(a, radial.y, b * tang.y), fmaf(a, radial.z, b * tang.z));
-    float len2 = dot3(local, local);
-    return len2 > 0.0f ? local * rsqrtf(len2) : radial;
+template <typename R> __device__ __forceinline__ V3<R> s_direction(const SLane<R>& l, R sn, R cs) {
+    V3<R> radial = v3<R>(fmaT(cs, l.e1.x, sn * l.e2.x), fmaT(cs, l.e1.y, sn * l.e2.y), fmaT(cs, l.e1.z, sn * l.e2.z));
+    V3<R> tang = v3<R>(fmaT(-sn, l.e1.x, cs * l.e2.x), fmaT(-sn, l.e1.y, cs * l.e2.y), fmaT(-sn, l.e1.z, cs * l.e2.z));
+    R a = l.s.rd * rsqrtT(gmax(R(1) - R(2) * rcp(l.s.r), R(1e-6)));
+    R b = l.s.r * l.s.pd;
+    V3<R> local = v3<R>(fmaT(a, radial.x, b * tang.x), fmaT(a, radial.y, b * tang.y), fmaT(a, radial.z, b * tang.z));
+    R len2 = dot(local, local);
+    return len2 > R(0) ? local * rsqrtT(len2) : radial;
 }
 
 // prepareRay (Geodesic.h:130-163) into a lane. Returns true when the ray is
 // sky-only; then *sky holds its asymptotic direction.
-__device__ __forceinline__ bool s_init(SLane& l, float3 origin, float3 direction, const MarchUniforms& u,
+template <typename R>
+__device__ __forceinline__ bool s_init(SLane<R>& l, float3 origin, float3 direction, const MarchUniforms& u,
                                        const SweepTables& t, float3* sky) {
-    PreparedRay<float> p = prepare_ray(to_v3<float>(origin), to_v3<float>(direction), u, t);
-    l.e1 = to_float3(p.ray.e1);
-    l.e2 = to_float3(p.ray.e2);
+    PreparedRay<R> p = prepare_ray(v3_of<R>(origin), v3_of<R>(direction), u, t);
+    l.e1 = p.ray.e1;
+    l.e2 = p.ray.e2;
     l.energy = p.ray.energy;
     l.angular_momentum = p.ray.angularMomentum;
     if (p.skyOnly) {
         *sky = to_float3(p.sky);
         return true;
     }
-    l.s = SState{p.ray.s.r, p.ray.s.phi, p.ray.s.vDot, p.ray.s.rDot, p.ray.s.phiDot};
-    l.c = SState{0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+    l.s = SState<R>{p.ray.s.r, p.ray.s.phi, p.ray.s.vDot, p.ray.s.rDot, p.ray.s.phiDot};
+    l.c = SState<R>{R(0), R(0), R(0), R(0), R(0)};
     double r0 = (double)l.s.r;
-    l.e0 = (float)((1.0 - 2.0 / r0) * (double)l.s.vd - (double)l.s.rd);
-    l.l0 = (float)(r0 * r0 * (double)l.s.pd);
+    l.e0 = (1.0 - 2.0 / r0) * (double)l.s.vd - (double)l.s.rd;
+    l.l0 = r0 * r0 * (double)l.s.pd;
     l.color = make_float3(0.0f, 0.0f, 0.0f);
     l.transmittance = 1.0f;
     l.travelled = l.weighted_depth = l.depth_weight = 0.0f;
-    float sn, cs;
+    R sn, cs;
     l.previous = s_position(l, &sn, &cs);
     l.steps = l.samples = 0;
     l.outcome = RayExhausted;
-    l.min_r = l.s.r;
+    l.min_r = (float)l.s.r;
     l.left_sphere = false;
     return false;
 }
 
-__device__ __forceinline__ void s_advance(SState& s, SState& c, float h) {
-    SState inc = s_increment(s, h);
-    comp_add(s.r, c.r, inc.r);
-    comp_add(s.phi, c.phi, inc.phi);
-    comp_add(s.vd, c.vd, inc.vd);
-    comp_add(s.rd, c.rd, inc.rd);
-    comp_add(s.pd, c.pd, inc.pd);
+template <typename R> __device__ __forceinline__ void s_advance(SState<R>& s, SState<R>& c, R h) {
+    SState<R> inc = s_increment(s, h);
+    comp_addT(s.r, c.r, inc.r);
+    comp_addT(s.phi, c.phi, inc.phi);
+    comp_addT(s.vd, c.vd, inc.vd);
+    comp_addT(s.rd, c.rd, inc.rd);
+    comp_addT(s.pd, c.pd, inc.pd);
 }
 
 // One iteration of marchRay's loop (march.metal:65-106). Returns true when
 // the ray ended (captured, escaped, left the sphere or hit the step cap).
-__device__ __forceinline__ bool s_step(SLane& l, const MarchUniforms& u, cudaTextureObject_t em, cudaTextureObject_t vel,
-                                       bool gather) {
+template <typename R>
+__device__ __forceinline__ bool s_step(SLane<R>& l, const MarchUniforms& u, cudaTextureObject_t em,
+                                       cudaTextureObject_t vel, bool gather) {
     const GeodesicSettings& g = u.geodesic;
     if (l.steps >= g.stepCap) return true;
-    float h = ray_step_length(l.previous.z, l.s.r, g);
-    const float sphere = u.sphereRadius;
-    SState before = l.s, before_c = l.c;
+    R h = ray_step_length(l.previous.z, l.s.r, g);
+    const R sphere = R(u.sphereRadius);
+    SState<R> before = l.s, before_c = l.c;
     s_advance(l.s, l.c, h);
     l.steps += 1u;
-    if (sphere > 0.0f && l.s.r >= sphere && l.s.rd > 0.0f && before.r < sphere) {
-        float frac = (sphere - before.r) / (l.s.r - before.r);
+    if (u.sphereRadius > 0.0f && l.s.r >= sphere && l.s.rd > R(0) && before.r < sphere) {
+        R frac = (sphere - before.r) / (l.s.r - before.r);
         l.s = before;
         l.c = before_c;
         s_advance(l.s, l.c, h * frac);
     }
-    float sn, cs;
-    float3 position = s_position(l, &sn, &cs);
-    float3 d = position - l.previous;
-    float path = sqrtf(dot3(d, d));
+    R sn, cs;
+    V3<R> position = s_position(l, &sn, &cs);
+    V3<R> d = position - l.previous;
+    float path = (float)gsqrt(dot(d, d));
     l.travelled += path;
-    l.min_r = fminf(l.min_r, l.s.r);
-    if (l.s.r <= g.captureRadius) {
+    l.min_r = fminf(l.min_r, (float)l.s.r);
+    if (l.s.r <= R(g.captureRadius)) {
         l.outcome = RayCaptured;
         return true;
     }
-    if (gather && in_slab(position, u.volumeHalfExtent) && l.transmittance > 0.004f) {
-        float f = fmaf(-2.0f, rcp(l.s.r), 1.0f);
-        float3 dir = s_direction(l, sn, cs);
-        gather_sample(gather_view(u, em, vel), position, f, dir, path, l.travelled, l.color, l.transmittance,
+    float3 pf = to_float3(position);
+    if (gather && in_slab(pf, u.volumeHalfExtent) && l.transmittance > 0.004f) {
+        float f = (float)fmaT(R(-2), rcp(l.s.r), R(1));
+        float3 dir = to_float3(s_direction(l, sn, cs));
+        gather_sample(gather_view(u, em, vel), pf, f, dir, path, l.travelled, l.color, l.transmittance,
                       l.weighted_depth, l.depth_weight, l.samples);
     }
     l.previous = position;
-    if (sphere > 0.0f && l.s.r >= sphere && l.s.rd > 0.0f) {
+    if (u.sphereRadius > 0.0f && l.s.r >= sphere && l.s.rd > R(0)) {
         l.outcome = RayEscaped;
         l.left_sphere = true;
         return true;
     }
-    if (l.s.r >= g.escapeRadius) {
+    if (l.s.r >= R(g.escapeRadius)) {
         l.outcome = RayEscaped;
         return true;
     }
     return false;
 }
 
-// Drift of the compensated state against its launch values (Geodesic.h:
-// 184-188), evaluated in double from value plus error word.
-__device__ __forceinline__ float s_drift(const SLane& l) {
+// Drift against the launch values (Geodesic.h:184-188), evaluated in double
+// from value plus error word.
+template <typename R> __device__ __forceinline__ float s_drift(const SLane<R>& l) {
     double r = (double)l.s.r + (double)l.c.r;
     double e = (1.0 - 2.0 / r) * ((double)l.s.vd + (double)l.c.vd) - ((double)l.s.rd + (double)l.c.rd);
     double lm = r * r * ((double)l.s.pd + (double)l.c.pd);
-    double ed = fabs(e - (double)l.e0) / fabs((double)l.e0);
-    double ld = fabs(lm - (double)l.l0) / fmax(fabs((double)l.l0), 1e-3);
+    double ed = fabs(e - l.e0) / fabs(l.e0);
+    double ld = fabs(lm - l.l0) / fmax(fabs(l.l0), 1e-3);
     return (float)fmax(ed, ld);
 }
 
-__device__ __forceinline__ bool s_falls_in(const SLane& l) {
+template <typename R> __device__ __forceinline__ bool s_falls_in(const SLane<R>& l) {
     return l.outcome == RayCaptured ||
-           (l.outcome == RayExhausted && l.s.rd < 0.0f && fabsf(l.angular_momentum) < B_CRITICAL * l.energy);
+           (l.outcome == RayExhausted && l.s.rd < R(0) && gabs(l.angular_momentum) < R(B_CRITICAL) * l.energy);
 }
 
 // Final sky direction: the sphere-exit asymptote or the last direction.
-__device__ __forceinline__ float3 s_sky(const SLane& l, const MarchUniforms& u, const SweepTables& t) {
-    float sn, cs;
+template <typename R>
+__device__ __forceinline__ V3<R> s_sky(const SLane<R>& l, const MarchUniforms& u, const SweepTables& t) {
+    R sn, cs;
     if (l.left_sphere) {
-        float b = fabsf(l.angular_momentum) / l.energy;
+        float b = (float)(gabs(l.angular_momentum) / l.energy);
         float sweep = sweep_lookup(t.sphere, 0.0f, u.sphereTableMaxB, b);
-        fast_sincos(l.s.phi + sweep, &sn, &cs);
-        return make_float3(fmaf(cs, l.e1.x, sn * l.e2.x), fmaf(cs, l.e1.y, sn * l.e2.y), fmaf(cs, l.e1.z, sn * l.e2.z));
+        fast_sincos(l.s.phi + R(sweep), &sn, &cs);
+        return v3<R>(fmaT(cs, l.e1.x, sn * l.e2.x), fmaT(cs, l.e1.y, sn * l.e2.y), fmaT(cs, l.e1.z, sn * l.e2.z));
     }
     fast_sincos(l.s.phi, &sn, &cs);
     return s_direction(l, sn, cs);
 }
 
-__device__ __forceinline__ PixelResult s_finish(const SLane& l, const MarchUniforms& u, const SweepTables& t,
+template <typename R>
+__device__ __forceinline__ PixelResult s_finish(const SLane<R>& l, const MarchUniforms& u, const SweepTables& t,
                                                 const float4* blackbody) {
     PixelResult r;
     r.color = l.color;
@@ -252,7 +323,7 @@ __device__ __forceinline__ PixelResult s_finish(const SLane& l, const MarchUnifo
     r.min_r = l.min_r;
     r.samples = l.samples;
     if (!s_falls_in(l) && u.starBrightness > 0.0f) {
-        float3 star = starfield(s_sky(l, u, t), u.starSeed, blackbody);
+        float3 star = starfield(to_float3(s_sky(l, u, t)), u.starSeed, blackbody);
         r.color = r.color + star * (l.transmittance * u.starBrightness);
     }
     return r;
@@ -273,16 +344,16 @@ __device__ __forceinline__ PixelResult sky_only_result(float3 sky, const MarchUn
 
 // --------------------------------------------------------------------- Kerr
 
-struct KState {
-    float r, th, ph, pr, pt;
+template <typename R> struct KState {
+    R r, th, ph, pr, pt;
 };
 
-struct KConst {
-    float a, a2, E, L, aE, aL, L2, a2E2, two_aEL;
+template <typename R> struct KConst {
+    R a, a2, E, L, aE, aL, L2, a2E2, two_aEL;
 };
 
-__device__ __forceinline__ KConst k_const(float a, float E, float L) {
-    KConst k;
+template <typename R> __device__ __forceinline__ KConst<R> k_const(R a, R E, R L) {
+    KConst<R> k;
     k.a = a;
     k.a2 = a * a;
     k.E = E;
@@ -291,164 +362,187 @@ __device__ __forceinline__ KConst k_const(float a, float E, float L) {
     k.aL = a * L;
     k.L2 = L * L;
     k.a2E2 = k.a2 * E * E;
-    k.two_aEL = 2.0f * a * E * L;
+    k.two_aEL = R(2) * a * E * L;
     return k;
 }
 
-// Hamilton's equations with the off-shell Sigma terms (Kerr.h:63-90).
-__device__ __forceinline__ KState k_derivative(const KConst& k, const KState& s) {
-    float st, ct;
-    fast_sincos(s.th, &st, &ct);
-    float r = s.r;
-    float r2 = r * r;
-    float delta = r2 - 2.0f * r + k.a2;
-    float sigma = fmaf(k.a2, ct * ct, r2);
-    float inv_sigma = rcp(sigma);
-    float inv_delta = rcp(delta);
-    float sin2 = fmaxf(st * st, 1e-8f);
-    float inv_sin2 = rcp(sin2);
-    float p = fmaf(r2 + k.a2, k.E, -k.aL);
-    float g = fmaf(k.a2E2, sin2, fmaf(k.L2, inv_sin2, -k.two_aEL));
-    float pr2 = s.pr * s.pr;
-    float p2d = p * p * inv_delta;
-    float F = fmaf(delta, pr2, fmaf(s.pt, s.pt, g - p2d));
-    float ham = 0.5f * F * inv_sigma;
-    float dprime = 2.0f * r - 2.0f;
-    float fr = fmaf(dprime, pr2, inv_delta * (p2d * dprime - 4.0f * r * k.E * p));
-    float fth = 2.0f * ct * fmaf(k.a2E2, st, -k.L2 * inv_sin2 * rcp(fmaxf(st, 1e-4f)));
-    KState o;
+// 1/max(sin^2, floor) and 1/max(sin, floor) (Kerr.h:32, :78). In FP32 the
+// floors are 1e-8 = (1e-4)^2 and 1e-4, so one reciprocal of max(|sin|,
+// 1e-4) gives both; the FP64 floors are the oracle's 1e-12 and 1e-9.
+template <typename R> __device__ __forceinline__ void k_sin_inverses(R st, R* inv_sin2, R* inv_sin_clamped) {
+    if constexpr (sizeof(R) == 4) {
+        R inv = rcp(fmaxf(fabsf(st), 1e-4f));
+        *inv_sin2 = inv * inv;
+        *inv_sin_clamped = st > 0.0f ? inv : 1e4f;
+    } else {
+        *inv_sin2 = rcp(fmax(st * st, 1e-12));
+        *inv_sin_clamped = rcp(fmax(st, 1e-9));
+    }
+}
+
+template <typename R> __device__ __forceinline__ R k_sin2(R st) { return gmax(st * st, R(sizeof(R) == 4 ? 1e-8 : 1e-12)); }
+
+// Hamilton's equations with the off-shell Sigma terms (Kerr.h:63-90), at a
+// polar angle whose sine and cosine are given.
+template <typename R>
+__device__ __forceinline__ KState<R> k_derivative(const KConst<R>& k, const KState<R>& s, R st, R ct) {
+    R r = s.r;
+    R r2 = r * r;
+    R delta = r2 - R(2) * r + k.a2;
+    R sigma = fmaT(k.a2, ct * ct, r2);
+    R inv_sigma = rcp(sigma);
+    R inv_delta = rcp(delta);
+    R sin2 = k_sin2(st);
+    R inv_sin2, inv_sc;
+    k_sin_inverses(st, &inv_sin2, &inv_sc);
+    R p = fmaT(r2 + k.a2, k.E, -k.aL);
+    R g = fmaT(k.a2E2, sin2, fmaT(k.L2, inv_sin2, -k.two_aEL));
+    R pr2 = s.pr * s.pr;
+    R p2d = p * p * inv_delta;
+    R F = fmaT(delta, pr2, fmaT(s.pt, s.pt, g - p2d));
+    R ham = R(0.5) * F * inv_sigma;
+    R dprime = R(2) * r - R(2);
+    R fr = fmaT(dprime, pr2, inv_delta * (p2d * dprime - R(4) * r * k.E * p));
+    R fth = R(2) * ct * fmaT(k.a2E2, st, -k.L2 * inv_sin2 * inv_sc);
+    KState<R> o;
     o.r = delta * s.pr * inv_sigma;
     o.th = s.pt * inv_sigma;
-    o.ph = (fmaf(k.a, p * inv_delta, k.L * inv_sin2) - k.aE) * inv_sigma;
-    o.pr = (2.0f * r * ham - 0.5f * fr) * inv_sigma;
-    o.pt = (-2.0f * k.a2 * st * ct * ham - 0.5f * fth) * inv_sigma;
+    o.ph = (fmaT(k.a, p * inv_delta, k.L * inv_sin2) - k.aE) * inv_sigma;
+    o.pr = (R(2) * r * ham - R(0.5) * fr) * inv_sigma;
+    o.pt = (R(-2) * k.a2 * st * ct * ham - R(0.5) * fth) * inv_sigma;
     return o;
 }
 
-__device__ __forceinline__ KState k_offset(const KState& s, const KState& d, float w) {
-    return KState{fmaf(d.r, w, s.r), fmaf(d.th, w, s.th), fmaf(d.ph, w, s.ph), fmaf(d.pr, w, s.pr), fmaf(d.pt, w, s.pt)};
+template <typename R> __device__ __forceinline__ KState<R> k_offset(const KState<R>& s, const KState<R>& d, R w) {
+    return KState<R>{fmaT(d.r, w, s.r), fmaT(d.th, w, s.th), fmaT(d.ph, w, s.ph), fmaT(d.pr, w, s.pr),
+                     fmaT(d.pt, w, s.pt)};
 }
 
-__device__ __forceinline__ KState k_increment(const KConst& k, const KState& s, float h) {
-    const float hh = 0.5f * h;
-    KState k1 = k_derivative(k, s);
-    KState k2 = k_derivative(k, k_offset(s, k1, hh));
-    KState k3 = k_derivative(k, k_offset(s, k2, hh));
-    KState k4 = k_derivative(k, k_offset(s, k3, h));
-    const float w = h * (1.0f / 6.0f);
-    KState inc;
-    inc.r = (k1.r + 2.0f * k2.r + (2.0f * k3.r + k4.r)) * w;
-    inc.th = (k1.th + 2.0f * k2.th + (2.0f * k3.th + k4.th)) * w;
-    inc.ph = (k1.ph + 2.0f * k2.ph + (2.0f * k3.ph + k4.ph)) * w;
-    inc.pr = (k1.pr + 2.0f * k2.pr + (2.0f * k3.pr + k4.pr)) * w;
-    inc.pt = (k1.pt + 2.0f * k2.pt + (2.0f * k3.pt + k4.pt)) * w;
-    return inc;
+// RK4 increment (Kerr.h:92-99); (st0, ct0) are sin and cos of s.th.
+template <typename R>
+__device__ __forceinline__ KState<R> k_increment(const KConst<R>& k, const KState<R>& s, R h, R st0, R ct0) {
+    KState<R> acc{R(0), R(0), R(0), R(0), R(0)};
+    KState<R> x = s;
+    R st = st0, ct = ct0;
+#pragma unroll 1
+    for (int stage = 0; stage < 4; ++stage) {
+        if (stage > 0) fast_sincos(x.th, &st, &ct);
+        KState<R> d = k_derivative(k, x, st, ct);
+        R wk = (stage == 0 || stage == 3) ? R(1) : R(2);
+        acc = k_offset(acc, d, wk);
+        x = k_offset(s, d, stage < 2 ? R(0.5) * h : h);
+    }
+    const R w = h * (R(1) / R(6));
+    return KState<R>{acc.r * w, acc.th * w, acc.ph * w, acc.pr * w, acc.pt * w};
 }
 
-struct KLane {
-    KState s, c;
-    KConst k;
-    float carter0, scale, capture, drift;
+template <typename R> struct KLane {
+    KState<R> s, c;
+    KConst<R> k;
+    R st, ct;  // sin and cos of s.th
+    R carter0, scale, capture;
+    float drift;
     float3 color;
     float transmittance, travelled, weighted_depth, depth_weight;
-    float3 previous;
+    V3<R> previous;
     uint32_t steps, samples, outcome;
     float min_r;
 };
 
-// Carter constant and null residual (Kerr.h:39-50) from the state.
-__device__ __forceinline__ void k_gauges(const KLane& l, float st, float ct, float* carter, float* residual) {
-    const KConst& k = l.k;
-    float sin2 = fmaxf(st * st, 1e-8f);
-    float inv_sin2 = rcp(sin2);
-    *carter = fmaf(ct * ct, fmaf(k.L2, inv_sin2, -k.a2E2), l.s.pt * l.s.pt);
-    float r = l.s.r;
-    float delta = r * r - 2.0f * r + k.a2;
-    float p = fmaf(r * r + k.a2, k.E, -k.aL);
-    float g = fmaf(k.a2E2, sin2, fmaf(k.L2, inv_sin2, -k.two_aEL));
-    *residual = fmaf(delta, l.s.pr * l.s.pr, fmaf(l.s.pt, l.s.pt, g - p * p * rcp(delta)));
+// Carter constant and null residual (Kerr.h:39-50) of the lane's state.
+template <typename R> __device__ __forceinline__ void k_gauges(const KLane<R>& l, R* carter, R* residual) {
+    const KConst<R>& k = l.k;
+    R sin2 = k_sin2(l.st);
+    R inv_sin2, inv_sc;
+    k_sin_inverses(l.st, &inv_sin2, &inv_sc);
+    *carter = fmaT(l.ct * l.ct, fmaT(k.L2, inv_sin2, -k.a2E2), l.s.pt * l.s.pt);
+    R r = l.s.r;
+    R delta = r * r - R(2) * r + k.a2;
+    R p = fmaT(r * r + k.a2, k.E, -k.aL);
+    R g = fmaT(k.a2E2, sin2, fmaT(k.L2, inv_sin2, -k.two_aEL));
+    *residual = fmaT(delta, l.s.pr * l.s.pr, fmaT(l.s.pt, l.s.pt, g - p * p * rcp(delta)));
 }
 
-__device__ __forceinline__ float3 k_position(const KLane& l, float st, float ct) {
-    float sp, cp;
+template <typename R> __device__ __forceinline__ V3<R> k_position(const KLane<R>& l) {
+    R sp, cp;
     fast_sincos(l.s.ph, &sp, &cp);
-    float radial = sqrtf(fmaf(l.s.r, l.s.r, l.k.a2));
-    return make_float3(radial * st * cp, radial * st * sp, l.s.r * ct);
+    R radial = gsqrt(fmaT(l.s.r, l.s.r, l.k.a2));
+    return v3<R>(radial * l.st * cp, radial * l.st * sp, l.s.r * l.ct);
 }
 
 // kerrLaunch (Kerr.h:110-148) into a lane.
-__device__ __forceinline__ void k_init(KLane& l, float3 origin, float3 direction, const MarchUniforms& u) {
-    const float a = u.spin;
-    KerrState<float> s0 = kerr_launch(a, to_v3<float>(origin), to_v3<float>(direction));
-    l.s = KState{s0.r, s0.theta, s0.phi, s0.pr, s0.ptheta};
-    l.c = KState{0.0f, 0.0f, 0.0f, 0.0f, 0.0f};
+template <typename R>
+__device__ __forceinline__ void k_init(KLane<R>& l, float3 origin, float3 direction, const MarchUniforms& u) {
+    const R a = R(u.spin);
+    KerrState<R> s0 = kerr_launch(a, v3_of<R>(origin), v3_of<R>(direction));
+    l.s = KState<R>{s0.r, s0.theta, s0.phi, s0.pr, s0.ptheta};
+    l.c = KState<R>{R(0), R(0), R(0), R(0), R(0)};
     l.k = k_const(a, s0.energy, s0.angularMomentum);
     l.carter0 = kerr_carter(a, s0);
-    l.scale = fmaxf(fabsf(l.carter0), s0.energy * s0.energy);
-    l.capture = kerr_outer_horizon(a) + KERR_CAPTURE_MARGIN;
+    l.scale = gmax(gabs(l.carter0), s0.energy * s0.energy);
+    l.capture = kerr_outer_horizon(a) + R(KERR_CAPTURE_MARGIN);
     l.drift = 0.0f;
     l.color = make_float3(0.0f, 0.0f, 0.0f);
     l.transmittance = 1.0f;
     l.travelled = l.weighted_depth = l.depth_weight = 0.0f;
-    float st, ct;
-    fast_sincos(l.s.th, &st, &ct);
-    l.previous = k_position(l, st, ct);
+    fast_sincos(l.s.th, &l.st, &l.ct);
+    l.previous = k_position(l);
     l.steps = l.samples = 0;
     l.outcome = RayExhausted;
-    l.min_r = l.s.r;
+    l.min_r = (float)l.s.r;
 }
 
 // One iteration of marchRayKerr's loop (march.metal:140-173).
-__device__ __forceinline__ bool k_step(KLane& l, const MarchUniforms& u, cudaTextureObject_t em, cudaTextureObject_t vel,
-                                       bool gather) {
+template <typename R>
+__device__ __forceinline__ bool k_step(KLane<R>& l, const MarchUniforms& u, cudaTextureObject_t em,
+                                       cudaTextureObject_t vel, bool gather) {
     const GeodesicSettings& g = u.geodesic;
     if (l.steps >= g.stepCap) return true;
     // kerrStepLength (Kerr.h:177-186)
-    float st0, ct0;
-    fast_sincos(l.s.th, &st0, &ct0);
-    float above = l.s.r - (l.capture - KERR_CAPTURE_MARGIN);
-    float pole = fminf(fmaxf(st0 * (1.0f / 0.08f), 0.05f), 1.0f);
-    float h = fminf(fmaxf(fminf(g.stepFactor * l.s.r, 0.2f * above) * pole, 0.002f), g.stepMax);
-    KState inc = k_increment(l.k, l.s, h);
-    comp_add(l.s.r, l.c.r, inc.r);
-    comp_add(l.s.th, l.c.th, inc.th);
-    comp_add(l.s.ph, l.c.ph, inc.ph);
-    comp_add(l.s.pr, l.c.pr, inc.pr);
-    comp_add(l.s.pt, l.c.pt, inc.pt);
+    R above = l.s.r - (l.capture - R(KERR_CAPTURE_MARGIN));
+    R pole = gmin(gmax(l.st * R(1.0 / 0.08), R(0.05)), R(1));
+    R h = gmin(gmax(gmin(R(g.stepFactor) * l.s.r, R(0.2) * above) * pole, R(0.002)), R(g.stepMax));
+    KState<R> inc = k_increment(l.k, l.s, h, l.st, l.ct);
+    comp_addT(l.s.r, l.c.r, inc.r);
+    comp_addT(l.s.th, l.c.th, inc.th);
+    comp_addT(l.s.ph, l.c.ph, inc.ph);
+    comp_addT(l.s.pr, l.c.pr, inc.pr);
+    comp_addT(l.s.pt, l.c.pt, inc.pt);
     l.steps += 1u;
-    float st, ct;
-    fast_sincos(l.s.th, &st, &ct);
-    float3 position = k_position(l, st, ct);
-    float3 d = position - l.previous;
-    float path = sqrtf(dot3(d, d));
+    fast_sincos(l.s.th, &l.st, &l.ct);
+    V3<R> position = k_position(l);
+    V3<R> d = position - l.previous;
+    float path = (float)gsqrt(dot(d, d));
     l.travelled += path;
-    float carter, residual;
-    k_gauges(l, st, ct, &carter, &residual);
-    float cd = fabsf(carter - l.carter0) / l.scale;
-    float nd = fabsf(residual) / (l.scale * fmaxf(l.s.r * l.s.r, 1.0f));
-    l.drift = fmaxf(l.drift, fmaxf(cd, nd));
-    l.min_r = fminf(l.min_r, l.s.r);
+    R carter, residual;
+    k_gauges(l, &carter, &residual);
+    R cd = gabs(carter - l.carter0) / l.scale;
+    R nd = gabs(residual) / (l.scale * gmax(l.s.r * l.s.r, R(1)));
+    l.drift = fmaxf(l.drift, (float)gmax(cd, nd));
+    l.min_r = fminf(l.min_r, (float)l.s.r);
     if (l.s.r <= l.capture) {
         l.outcome = RayCaptured;
         return true;
     }
-    if (gather && in_slab(position, u.volumeHalfExtent) && l.transmittance > 0.004f) {
-        float sigma = fmaf(l.k.a2, ct * ct, l.s.r * l.s.r);
-        float fk = 1.0f - 2.0f * l.s.r / sigma;
-        KerrState<float> ks{l.s.r, l.s.th, l.s.ph, l.s.pr, l.s.pt, l.k.E, l.k.L};
+    float3 pf = to_float3(position);
+    if (gather && in_slab(pf, u.volumeHalfExtent) && l.transmittance > 0.004f) {
+        R sigma = fmaT(l.k.a2, l.ct * l.ct, l.s.r * l.s.r);
+        float fk = (float)(R(1) - R(2) * l.s.r * rcp(sigma));
+        KerrState<R> ks{l.s.r, l.s.th, l.s.ph, l.s.pr, l.s.pt, l.k.E, l.k.L};
         float3 dir = to_float3(kerr_direction(l.k.a, ks));
-        gather_sample(gather_view(u, em, vel), position, fmaxf(fk, 0.0f), dir, path, l.travelled, l.color,
+        gather_sample(gather_view(u, em, vel), pf, fmaxf(fk, 0.0f), dir, path, l.travelled, l.color,
                       l.transmittance, l.weighted_depth, l.depth_weight, l.samples);
     }
     l.previous = position;
-    if (l.s.r >= g.escapeRadius) {
+    if (l.s.r >= R(g.escapeRadius)) {
         l.outcome = RayEscaped;
         return true;
     }
     return false;
 }
 
-__device__ __forceinline__ PixelResult k_finish(const KLane& l, const MarchUniforms& u, const float4* blackbody) {
+template <typename R>
+__device__ __forceinline__ PixelResult k_finish(const KLane<R>& l, const MarchUniforms& u, const float4* blackbody) {
     PixelResult r;
     r.color = l.color;
     r.drift = l.drift;
@@ -457,9 +551,9 @@ __device__ __forceinline__ PixelResult k_finish(const KLane& l, const MarchUnifo
     r.depth = l.depth_weight > 0.0f ? l.weighted_depth / l.depth_weight : l.travelled;
     r.min_r = l.min_r;
     r.samples = l.samples;
-    bool falls_in = l.outcome == RayCaptured || (l.outcome == RayExhausted && l.s.pr < 0.0f);
+    bool falls_in = l.outcome == RayCaptured || (l.outcome == RayExhausted && l.s.pr < R(0));
     if (!falls_in && u.starBrightness > 0.0f) {
-        KerrState<float> ks{l.s.r, l.s.th, l.s.ph, l.s.pr, l.s.pt, l.k.E, l.k.L};
+        KerrState<R> ks{l.s.r, l.s.th, l.s.ph, l.s.pr, l.s.pt, l.k.E, l.k.L};
         float3 star = starfield(to_float3(kerr_direction(l.k.a, ks)), u.starSeed, blackbody);
         r.color = r.color + star * (l.transmittance * u.starBrightness);
     }
@@ -467,13 +561,14 @@ __device__ __forceinline__ PixelResult k_finish(const KLane& l, const MarchUnifo
 }
 
 // probeRays' result fields (march.metal:303-340) from a finished lane.
-__device__ inline RayProbeResult s_probe_result(const SLane& l, const MarchUniforms& u, const SweepTables& t) {
+template <typename R>
+__device__ inline RayProbeResult s_probe_result(const SLane<R>& l, const MarchUniforms& u, const SweepTables& t) {
     RayProbeResult out;
-    float sn, cs;
-    float3 pos = s_position(l, &sn, &cs);
-    float3 dir = (l.outcome == RayEscaped && !s_falls_in(l)) ? s_sky(l, u, t) : s_direction(l, sn, cs);
-    out.position = {pos.x, pos.y, pos.z};
-    out.direction = {dir.x, dir.y, dir.z};
+    R sn, cs;
+    V3<R> pos = s_position(l, &sn, &cs);
+    V3<R> dir = (l.outcome == RayEscaped && !s_falls_in(l)) ? s_sky(l, u, t) : s_direction(l, sn, cs);
+    out.position = {(float)pos.x, (float)pos.y, (float)pos.z};
+    out.direction = {(float)dir.x, (float)dir.y, (float)dir.z};
     out.drift = s_drift(l);
     out.outcome = l.outcome;
     out.steps = l.steps;
@@ -483,42 +578,45 @@ __device__ inline RayProbeResult s_probe_result(const SLane& l, const MarchUnifo
     return out;
 }
 
-__device__ inline RayProbeResult k_probe_result(const KLane& l) {
+template <typename R> __device__ inline RayProbeResult k_probe_result(const KLane<R>& l) {
     RayProbeResult out;
-    float st, ct;
-    fast_sincos(l.s.th, &st, &ct);
-    float3 pos = k_position(l, st, ct);
-    KerrState<float> ks{l.s.r, l.s.th, l.s.ph, l.s.pr, l.s.pt, l.k.E, l.k.L};
-    float3 dir = to_float3(kerr_direction(l.k.a, ks));
-    out.position = {pos.x, pos.y, pos.z};
-    out.direction = {dir.x, dir.y, dir.z};
+    V3<R> pos = k_position(l);
+    KerrState<R> ks{l.s.r, l.s.th, l.s.ph, l.s.pr, l.s.pt, l.k.E, l.k.L};
+    V3<R> dir = kerr_direction(l.k.a, ks);
+    out.position = {(float)pos.x, (float)pos.y, (float)pos.z};
+    out.direction = {(float)dir.x, (float)dir.y, (float)dir.z};
     out.drift = l.drift;
     out.outcome = l.outcome;
     out.steps = l.steps;
-    out.energy = l.k.E;
-    out.angularMomentum = l.k.L;
+    out.energy = (float)l.k.E;
+    out.angularMomentum = (float)l.k.L;
     return out;
 }
 
-// One pixel through the compensated path, run to completion.
-__device__ inline PixelResult shade_pixel_compensated(const MarchParams& p, uint32_t px, uint32_t py) {
+// One pixel through the lane path, run to completion: compensated FP32, or
+// the FP64 re-integration with R = double.
+template <typename R> __device__ inline PixelResult shade_pixel_lane(const MarchParams& p, uint32_t px, uint32_t py) {
     const MarchUniforms& u = p.u;
     const bool gather = p.emission != 0;
     float3 dir = camera_direction(u, px, py);
     float3 origin = to_f3(u.cameraPosition);
     if (u.spin > 0.0f) {
-        KLane l;
+        KLane<R> l;
         k_init(l, origin, dir, u);
         for (uint32_t k = 0; k <= STEP_CAP_STILL; ++k)
             if (k_step(l, u, p.emission, p.velocity, gather)) break;
         return k_finish(l, u, p.blackbody);
     }
-    SLane l;
+    SLane<R> l;
     float3 sky;
     if (s_init(l, origin, dir, u, p.tables, &sky)) return sky_only_result(sky, u, p.blackbody);
     for (uint32_t k = 0; k <= STEP_CAP_STILL; ++k)
         if (s_step(l, u, p.emission, p.velocity, gather)) break;
     return s_finish(l, u, p.tables, p.blackbody);
+}
+
+__device__ inline PixelResult shade_pixel_compensated(const MarchParams& p, uint32_t px, uint32_t py) {
+    return shade_pixel_lane<float>(p, px, py);
 }
 
 }  // namespace gg

@@ -58,7 +58,7 @@ __global__ void __launch_bounds__(128) reintegrate_kernel(MarchParams p) {
     for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const uint32_t local = p.flagged[i];
         const uint32_t gx = local % p.target_width, gy = local / p.target_width;
-        PixelResult r = shade_pixel<double, false>(p, p.u.tileOrigin.x + gx, p.u.tileOrigin.y + gy);
+        PixelResult r = shade_pixel_lane<double>(p, p.u.tileOrigin.x + gx, p.u.tileOrigin.y + gy);
         write_pixel(p, local, r);
         atomicAdd(&p.stats[2], 1ull);
     }
@@ -128,14 +128,14 @@ __global__ void __launch_bounds__(64) probe_kernel(MarchParams p, const RayProbe
         float3 origin = make_float3(q.origin.x, q.origin.y, q.origin.z);
         float3 dir = make_float3(q.direction.x, q.direction.y, q.direction.z);
         if (u.spin > 0.0f) {
-            KLane l;
+            KLane<float> l;
             k_init(l, origin, dir, u);
             for (uint32_t k = 0; k <= STEP_CAP_STILL; ++k)
                 if (k_step(l, u, 0, 0, false)) break;
             r = k_probe_result(l);
             min_r = l.min_r;
         } else {
-            SLane l;
+            SLane<float> l;
             float3 sky;
             if (s_init(l, origin, dir, u, p.tables, &sky)) {
                 r = probe_one<float, false>(p, q, &min_r);  // sky-only: no integration either way

@@ -132,8 +132,8 @@ __device__ __forceinline__ void complete(const WaveArgs& a, uint32_t req, uint32
 }
 
 template <int Kind> struct LaneOf;
-template <> struct LaneOf<0> { typedef SLane type; };
-template <> struct LaneOf<1> { typedef KLane type; };
+template <> struct LaneOf<0> { typedef SLane<float> type; };
+template <> struct LaneOf<1> { typedef KLane<float> type; };
 
 template <int Kind>
 __device__ void serve_queue(const WaveArgs& a, uint32_t lane) {
@@ -230,16 +230,13 @@ __device__ void serve_queue(const WaveArgs& a, uint32_t lane) {
     }
 }
 
-__global__ void __launch_bounds__(kServeThreads) serve_kernel(WaveArgs a) {
-    const uint32_t lane = threadIdx.x & 31u;
-    const uint32_t warp = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    if (warp & 1u) {
-        serve_queue<1>(a, lane);
-        serve_queue<0>(a, lane);
-    } else {
-        serve_queue<0>(a, lane);
-        serve_queue<1>(a, lane);
-    }
+// One persistent kernel per metric; a wave runs both side by side.
+__global__ void __launch_bounds__(kServeThreads) serve_schwarzschild_kernel(WaveArgs a) {
+    serve_queue<0>(a, threadIdx.x & 31u);
+}
+
+__global__ void __launch_bounds__(kServeThreads) serve_kerr_kernel(WaveArgs a) {
+    serve_queue<1>(a, threadIdx.x & 31u);
 }
 
 // FP64 re-integration of the wave's flagged rays.
@@ -256,7 +253,7 @@ __global__ void __launch_bounds__(128) serve_reintegrate_kernel(WaveArgs a) {
         p.velocity = a.velocity;
         p.blackbody = a.blackbody;
         uint32_t w = R.u.resolution.x;
-        PixelResult r = shade_pixel<double, false>(p, pixel % w, pixel / w);
+        PixelResult r = shade_pixel_lane<double>(p, pixel % w, pixel / w);
         write_result(R, pixel, r);
         atomicAdd(R.stats + 2, 1ull);
     }
@@ -338,6 +335,10 @@ struct ServedRequest {
 
 struct WaveSlot {
     cudaStream_t stream = nullptr;
+    cudaStream_t side = nullptr;   // second branch of the wave graph
+    cudaStream_t fp64 = nullptr;   // the FP64 re-integration pass
+    cudaEvent_t fork = nullptr, join = nullptr;
+    cudaEvent_t fp64_done = nullptr;
     cudaEvent_t start = nullptr, stop = nullptr;
     cudaGraphExec_t graph = nullptr;
     char* device = nullptr;  // header, requests, chunks0, chunks1, flagged
@@ -357,7 +358,7 @@ struct gg_server {
     uint32_t max_chunks = 0;
     uint32_t flagged_capacity = 0;
     uint64_t slot_bytes = 0;
-    int grid = 0;
+    int grid_s = 0, grid_k = 0;
     cudaStream_t build = nullptr, copy = nullptr, plain = nullptr;
     cudaEvent_t built = nullptr, origin = nullptr;
     std::vector<gg::WaveSlot> slots;
@@ -384,11 +385,18 @@ static uint64_t slot_offset_chunks0(const gg_server* s) { return slot_offset_req
 static uint64_t slot_offset_chunks1(const gg_server* s) { return slot_offset_chunks0(s) + (uint64_t)s->max_chunks * sizeof(ServeChunk); }
 static uint64_t slot_offset_flagged(const gg_server* s) { return slot_offset_chunks1(s) + (uint64_t)s->max_chunks * sizeof(ServeChunk); }
 
+// The wave graph: fork, the Schwarzschild and Kerr persistent kernels side
+// by side, join. The FP64 pass is launched outside the graph on its own
+// stream so it overlaps the next wave.
 static int capture_wave_graph(gg_server* s, WaveSlot& w) {
     cudaGraph_t g = nullptr;
     GG_CUDA(cudaStreamBeginCapture(w.stream, cudaStreamCaptureModeThreadLocal), "wave capture");
-    serve_kernel<<<s->grid, kServeThreads, 0, w.stream>>>(w.args);
-    serve_reintegrate_kernel<<<s->ctx->sm_count * 2, 128, 0, w.stream>>>(w.args);
+    GG_CUDA(cudaEventRecord(w.fork, w.stream), "wave capture");
+    GG_CUDA(cudaStreamWaitEvent(w.side, w.fork, 0), "wave capture");
+    serve_schwarzschild_kernel<<<s->grid_s, kServeThreads, 0, w.side>>>(w.args);
+    serve_kerr_kernel<<<s->grid_k, kServeThreads, 0, w.stream>>>(w.args);
+    GG_CUDA(cudaEventRecord(w.join, w.side), "wave capture");
+    GG_CUDA(cudaStreamWaitEvent(w.stream, w.join, 0), "wave capture");
     cudaError_t e = cudaStreamEndCapture(w.stream, &g);
     GG_CUDA(e, "wave capture");
     e = cudaGraphInstantiate(&w.graph, g, 0);
@@ -514,19 +522,28 @@ static int launch_wave(gg_server* s, WaveSlot& w) {
     GG_CUDA(cudaEventRecord(w.start, w.stream), "wave event");
     GG_CUDA(cudaGraphLaunch(w.graph, w.stream), "wave launch");
     GG_CUDA(cudaEventRecord(w.stop, w.stream), "wave event");
+    // FP64 pass after the wave, on its own stream: it overlaps the next wave.
+    GG_CUDA(cudaStreamWaitEvent(w.fp64, w.stop, 0), "FP64 ordering");
+    serve_reintegrate_kernel<<<s->ctx->sm_count * 2, 128, 0, w.fp64>>>(w.args);
+    GG_CHECK(launch_status("FP64 re-integration"));
+    GG_CUDA(cudaEventRecord(w.fp64_done, w.fp64), "wave event");
     w.busy = true;
     s->total_waves += 1;
     return GG_OK;
 }
 
 static int finish_wave(gg_server* s, WaveSlot& w) {
-    float t0 = 0.0f, t1 = 0.0f;
+    // The wave's device interval runs from its start to the end of its FP64
+    // pass, which may overlap the next wave.
+    float t0 = 0.0f, t1 = 0.0f, t2 = 0.0f;
     GG_CUDA(cudaEventElapsedTime(&t0, s->origin, w.start), "wave timing");
     GG_CUDA(cudaEventElapsedTime(&t1, s->origin, w.stop), "wave timing");
+    GG_CUDA(cudaEventElapsedTime(&t2, s->origin, w.fp64_done), "wave timing");
+    t1 = std::max(t1, t2);
     s->intervals.emplace_back((double)t0 * 1e-3, (double)t1 * 1e-3);
     for (auto& r : w.members) {
         r->waves_pending -= 1;
-        if (r->waves_pending == 0 && r->next_ray >= r->rays && !r->copying) GG_CHECK(start_copy(s, *r, w.stop));
+        if (r->waves_pending == 0 && r->next_ray >= r->rays && !r->copying) GG_CHECK(start_copy(s, *r, w.fp64_done));
     }
     w.members.clear();
     w.busy = false;
@@ -625,7 +642,7 @@ static void worker_loop(gg_server* s) {
         bool any_busy = false;
         for (auto& w : s->slots) {
             if (!w.busy || status != GG_OK) continue;
-            cudaError_t q = cudaEventQuery(w.stop);
+            cudaError_t q = cudaEventQuery(w.fp64_done);
             if (q == cudaSuccess) status = finish_wave(s, w);
             else if (q != cudaErrorNotReady) status = cuda_status(q, "wave");
             else any_busy = true;
@@ -687,7 +704,7 @@ GG_API int gg_server_create(gg_context* ctx, const gg_volume* vol, const gg_serv
         return gg::fail(GG_ERR_OVER_BUDGET, "The server asks for %llu bytes but the budget has %llu left.",
                         (unsigned long long)s->cfg.memory_bytes, (unsigned long long)(ctx->budget - ctx->used));
     if (s->cfg.wave_rays == 0) s->cfg.wave_rays = 4u << 20;
-    if (s->cfg.chunk_rays == 0) s->cfg.chunk_rays = 256;
+    if (s->cfg.chunk_rays == 0) s->cfg.chunk_rays = 32;
     if (s->cfg.max_waves_in_flight == 0) s->cfg.max_waves_in_flight = 2;
     if (s->cfg.max_waves_in_flight > 4) s->cfg.max_waves_in_flight = 4;
     if (s->cfg.chunk_rays < 32 || s->cfg.chunk_rays > 65536)
@@ -696,8 +713,11 @@ GG_API int gg_server_create(gg_context* ctx, const gg_volume* vol, const gg_serv
     s->flagged_capacity = s->cfg.wave_rays / 8;
     s->slot_bytes = gg::slot_offset_flagged(s.get()) + (uint64_t)s->flagged_capacity * 8u;
     int blocks = 0;
-    GG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, gg::serve_kernel, gg::kServeThreads, 0), "occupancy");
-    s->grid = std::max(1, blocks) * ctx->sm_count;
+    GG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, gg::serve_schwarzschild_kernel, gg::kServeThreads, 0),
+            "occupancy");
+    s->grid_s = std::max(1, blocks) * ctx->sm_count;
+    GG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, gg::serve_kerr_kernel, gg::kServeThreads, 0), "occupancy");
+    s->grid_k = std::max(1, blocks) * ctx->sm_count;
     GG_CUDA(cudaStreamCreateWithFlags(&s->build, cudaStreamNonBlocking), "server streams");
     GG_CUDA(cudaStreamCreateWithFlags(&s->copy, cudaStreamNonBlocking), "server streams");
     GG_CUDA(cudaStreamCreateWithFlags(&s->plain, cudaStreamNonBlocking), "server streams");
@@ -709,6 +729,11 @@ GG_API int gg_server_create(gg_context* ctx, const gg_volume* vol, const gg_serv
     s->slots.resize(nslots);
     for (auto& w : s->slots) {
         GG_CUDA(cudaStreamCreateWithFlags(&w.stream, cudaStreamNonBlocking), "wave stream");
+        GG_CUDA(cudaStreamCreateWithFlags(&w.side, cudaStreamNonBlocking), "wave stream");
+        GG_CUDA(cudaStreamCreateWithFlags(&w.fp64, cudaStreamNonBlocking), "wave stream");
+        GG_CUDA(cudaEventCreateWithFlags(&w.fork, cudaEventDisableTiming), "wave events");
+        GG_CUDA(cudaEventCreateWithFlags(&w.join, cudaEventDisableTiming), "wave events");
+        GG_CUDA(cudaEventCreate(&w.fp64_done), "wave events");
         GG_CUDA(cudaEventCreate(&w.start), "wave events");
         GG_CUDA(cudaEventCreate(&w.stop), "wave events");
         if (s->cfg.mode == GG_SERVE_SERIAL_PLAIN) continue;
@@ -748,8 +773,14 @@ GG_API void gg_server_destroy(gg_server* s) {
         if (w.graph) cudaGraphExecDestroy(w.graph);
         if (w.device) gg::device_free(ctx, w.device, s->slot_bytes);
         if (w.host) cudaFreeHost(w.host);
+        if (w.fp64) cudaStreamSynchronize(w.fp64);
         if (w.start) cudaEventDestroy(w.start);
         if (w.stop) cudaEventDestroy(w.stop);
+        if (w.fork) cudaEventDestroy(w.fork);
+        if (w.join) cudaEventDestroy(w.join);
+        if (w.fp64_done) cudaEventDestroy(w.fp64_done);
+        if (w.side) cudaStreamDestroy(w.side);
+        if (w.fp64) cudaStreamDestroy(w.fp64);
         if (w.stream) cudaStreamDestroy(w.stream);
     }
     cudaStreamSynchronize(s->copy);

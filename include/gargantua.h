@@ -306,7 +306,7 @@ typedef struct {
     int mode;                  /* gg_serve_mode */
     uint64_t memory_bytes;     /* device memory for admitted requests' targets; 0: a quarter of the budget left */
     uint32_t wave_rays;        /* rays packed into one persistent launch; 0: 4 Mi */
-    uint32_t chunk_rays;       /* rays per work-stealing chunk; 0: 256 */
+    uint32_t chunk_rays;       /* rays per work-stealing chunk; 0: 32, one per lane of a warp */
     uint32_t max_waves_in_flight; /* 0: 2 */
 } gg_server_config;
 
