@@ -82,6 +82,7 @@ SIGNATURES = {
     "gg_march": (i, [vp, vp, P(T.MarchUniforms), vp, i, P(T.MarchCounters)]),
     "gg_probe": (i, [vp, P(T.MarchUniforms), vp, vp, u32, i]),
     "gg_march_stats": (i, [vp, P(u64), P(u64), P(u64)]),
+    "gg_march_compensated_noalloc": (i, [vp, vp, P(T.MarchUniforms), vp, P(T.MarchCounters)]),
     "gg_bake_create": (i, [vp, u32, u32, P(vp)]),
     "gg_bake_destroy": (None, [vp]),
     "gg_bake_rows": (i, [vp, P(T.MarchUniforms), u32, u32]),

@@ -165,6 +165,18 @@ MarchParams make_params(gg_context* ctx, const gg_volume* vol, const MarchUnifor
     return p;
 }
 
+// The compensated image march and its FP64 pass, given a parameter block
+// whose flagged list and counter are already set (p.flagged, p.flagged_count
+// zeroed by the caller, p.flagged_capacity entries).
+int launch_compensated_image(const MarchParams& p, cudaStream_t stream, int sm_count) {
+    dim3 block(MARCH_THREADGROUP_WIDTH, MARCH_THREADGROUP_HEIGHT);
+    dim3 grid((p.target_width + block.x - 1) / block.x, (p.target_height + block.y - 1) / block.y);
+    march_image_kernel<true><<<grid, block, 0, stream>>>(p);
+    GG_CHECK(launch_status("compensated march"));
+    reintegrate_kernel<<<sm_count, 128, 0, stream>>>(p);
+    return launch_status("FP64 re-integration");
+}
+
 int launch_plain_image(const MarchParams& p, cudaStream_t stream) {
     dim3 block(MARCH_THREADGROUP_WIDTH, MARCH_THREADGROUP_HEIGHT);
     dim3 grid((p.target_width + block.x - 1) / block.x, (p.target_height + block.y - 1) / block.y);

@@ -218,6 +218,27 @@ GG_API int gg_march_stats(gg_context* ctx, uint64_t* ray_steps, uint64_t* sample
 GG_API int gg_probe(gg_context* ctx, const MarchUniforms* u, const RayProbe* probes, RayProbeResult* results,
                     uint32_t count, int precision);
 
+/* Largest target, in pixels, gg_march_compensated_noalloc serves. */
+#define NOALLOC_MAX_PIXELS 2097152u
+
+/* The compensated march of gg_march (GG_PRECISION_COMPENSATED) for callers
+ * that must not allocate device memory once they run: hosts whose device
+ * memory is handed to their own pool up front, frame loops that cannot
+ * absorb cudaMalloc/cudaFree (cudaFree synchronises the device) or an
+ * allocation failure mid-frame, plugins inside a program that owns the
+ * memory budget. It allocates nothing: the FP64 re-integration list lives in
+ * a fixed device array of NOALLOC_MAX_PIXELS + 64 words (about 8 MiB) that
+ * every GPU loading the library holds until exit, and targets larger than
+ * NOALLOC_MAX_PIXELS are refused with GG_ERR_INVALID_ARGUMENT. The caller
+ * passes inputs and outputs as for gg_march (sweep tables, when enabled,
+ * come from an earlier gg_tables_update). The first call on each device
+ * looks up the array's device address; make it before any stream capture.
+ * All calls on a device share the array: calls whose work overlaps on the
+ * GPU race, so serialise them. This entry point has no counterpart in the
+ * reference, whose host allocates every buffer up front. */
+GG_API int gg_march_compensated_noalloc(gg_context* ctx, const gg_volume* vol, const MarchUniforms* u,
+                                        gg_targets* targets, MarchCounters* counters);
+
 /* ------------------------------------------------------------ bake / walk */
 
 /* Bake storage for width x height rays: BAKE_SAMPLES half4 samples per ray
