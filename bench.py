@@ -215,11 +215,21 @@ def cpu_sample(slices, seconds: float, threads: int):
     return total_steps / max(elapsed, 1e-9), total_rays, total_steps, elapsed, desc
 
 
-def setup_world(device: int):
+def setup_world(device: int, world: int):
     import gargantua_b200 as g
 
     # A server-sized budget: the reference's 3 GB cap is a laptop rule.
     ctx = g.Context(device, budget_bytes=48 << 30)
+    if world > 1:
+        # The disk's particles are sharded over the ranks and their grids
+        # summed over NCCL, so every rank serves the same volume.
+        from gargantua_b200 import parallel
+
+        disk = parallel.ShardedDisk(ctx, 1_000_000, 128, seed=1)
+        disk.advance(300, seed_first=True)  # STILL_SETTLE_STEPS = 600 substeps
+        disk.splat(exact=True)
+        ctx.synchronize()
+        return ctx, disk, disk.volume
     ps = g.Particles(ctx, 1_000_000, seed=1)
     ps.advance(300, seed_first=True)  # STILL_SETTLE_STEPS = 600 substeps
     vol = g.Volume(ctx, 128)
@@ -290,7 +300,7 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
     import gargantua_b200 as g
 
-    ctx, ps, vol = setup_world(local)
+    ctx, ps, vol = setup_world(local, world)
     peak = ctx.fp32_peak_tflops()
     # Weak scaling: every rank serves its own stream (seed 1 + rank).
     stream = make_stream(1 + rank)

@@ -58,6 +58,7 @@ SIGNATURES = {
     "gg_context_blackbody": (i, [vp, f32p, u32]),
     "gg_particles_create": (i, [vp, u32, u64, u32, P(vp)]),
     "gg_particles_destroy": (None, [vp]),
+    "gg_particles_create_shard": (i, [vp, u32, u32, u64, u32, P(vp)]),
     "gg_particles_uniforms": (i, [vp, P(T.SimUniforms)]),
     "gg_particles_seed": (i, [vp]),
     "gg_particles_step": (i, [vp, u32]),
@@ -72,6 +73,8 @@ SIGNATURES = {
     "gg_splat_resolve": (i, [vp, P(T.SplatUniforms), vp]),
     "gg_volume_clear": (i, [vp]),
     "gg_volume_read_sums": (i, [vp, vp, vp, vp]),
+    "gg_volume_write_sums": (i, [vp, vp, vp, vp]),
+    "gg_volume_sums": (i, [vp, P(vp), P(u64)]),
     "gg_volume_read": (i, [vp, vp, vp]),
     "gg_volume_write": (i, [vp, vp, vp]),
     "gg_tables_update": (i, [vp, C.c_float, P(T.MarchUniforms)]),

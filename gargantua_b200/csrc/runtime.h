@@ -107,6 +107,7 @@ int blackbody_init(gg_context* ctx);
 struct gg_particles {
     gg_context* ctx = nullptr;
     uint32_t count = 0;
+    uint32_t first_index = 0;  // global index of slot 0 (shards of a larger system)
     uint64_t seed = 0;
     uint32_t potential = PotentialPaczynskiWiita;
     float4* pos = nullptr;  // x, y, z, temperature

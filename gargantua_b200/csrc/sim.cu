@@ -26,6 +26,7 @@ struct SimArgs {
     float4* __restrict__ vel;
     const float* __restrict__ inverse_cdf;
     SimUniforms u;
+    uint32_t first_index;  // global index of slot 0: the hash is keyed on global indices
 };
 
 // Unnormalized thin-disk profile (Common.h:49-53) with the powers as square
@@ -87,7 +88,7 @@ __global__ void __launch_bounds__(256) seed_kernel(SimArgs a) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= a.u.particleCount) return;
     float4 p, v;
-    spawn(i, 0u, a, true, p, v);
+    spawn(a.first_index + i, 0u, a, true, p, v);
     a.pos[i] = p;
     a.vel[i] = v;
 }
@@ -129,7 +130,7 @@ __global__ void __launch_bounds__(256) step_kernel(SimArgs a) {
         float closest = len3(bx + along * tx, by + along * ty, bz + along * tz);
         if (closest < R_CAPTURE || r > R_ESCAPE || len3(vx, vy, vz) > PLUNGE_SPEED_LIMIT) {
             float4 np, nv;
-            spawn(i, __float_as_uint(v.w) + 1u, a, false, np, nv);
+            spawn(a.first_index + i, __float_as_uint(v.w) + 1u, a, false, np, nv);
             px = np.x; py = np.y; pz = np.z;
             vx = nv.x; vy = nv.y; vz = nv.z;
             v.w = nv.w;
@@ -155,6 +156,7 @@ static SimArgs sim_args(gg_particles* ps) {
     a.vel = ps->vel;
     a.inverse_cdf = ps->inverse_cdf;
     a.u = ps->uniforms;
+    a.first_index = ps->first_index;
     return a;
 }
 
@@ -162,7 +164,15 @@ extern "C" {
 
 GG_API int gg_particles_create(gg_context* ctx, uint32_t count, uint64_t seed, uint32_t potential,
                                gg_particles** out) {
+    return gg_particles_create_shard(ctx, count, 0u, seed, potential, out);
+}
+
+GG_API int gg_particles_create_shard(gg_context* ctx, uint32_t count, uint32_t first_index, uint64_t seed,
+                                     uint32_t potential, gg_particles** out) {
     if (!ctx || !out) return gg::fail(GG_ERR_INVALID_ARGUMENT, "gg_particles_create needs a context and an output.");
+    if ((uint64_t)first_index + count > 0xffffffffull)
+        return gg::fail(GG_ERR_INVALID_ARGUMENT, "Shard [%u, %u + %u) exceeds 32-bit particle indices.", first_index,
+                        first_index, count);
     *out = nullptr;
     if (count == 0) return gg::fail(GG_ERR_INVALID_ARGUMENT, "A particle system needs at least one particle.");
     if (potential != PotentialNewtonian && potential != PotentialPaczynskiWiita)
@@ -176,6 +186,7 @@ GG_API int gg_particles_create(gg_context* ctx, uint32_t count, uint64_t seed, u
     gg_particles* ps = new gg_particles();
     ps->ctx = ctx;
     ps->count = count;
+    ps->first_index = first_index;
     ps->seed = seed;
     ps->potential = potential;
     int s = gg::device_alloc(ctx, (uint64_t)count * 16u, (void**)&ps->pos, "particle positions");

@@ -29,6 +29,7 @@ struct SplatArgs {
     const float4* __restrict__ vel;
     uint32_t* __restrict__ sums;
     SplatUniforms u;
+    uint32_t first_index;  // global index of slot 0, for the stochastic pick
 };
 
 // One corner's six fixed-point atomics (splat.metal:25-37).
@@ -57,6 +58,7 @@ __global__ void __launch_bounds__(256) bin_kernel(SplatArgs a) {
     const SplatUniforms& u = a.u;
     if (i >= u.particleCount) return;
     float4 p = a.pos[i];
+    const uint32_t gi = a.first_index + i;
     float ux = (p.x + u.halfExtent) / (2.0f * u.halfExtent);
     float uy = (p.y + u.halfExtent) / (2.0f * u.halfExtent);
     float uz = (p.z + u.halfExtent) / (2.0f * u.halfExtent);
@@ -87,7 +89,7 @@ __global__ void __launch_bounds__(256) bin_kernel(SplatArgs a) {
             deposit(a.sums, index, w, energy, relative, v.x, v.y, v.z);
         }
     } else {
-        uint4 h = pcg4d(make_uint4(i, u.frame, u.seed.x, u.seed.y));
+        uint4 h = pcg4d(make_uint4(gi, u.frame, u.seed.x, u.seed.y));
         int cx = unit_float(h.x) < fx ? hx : lx;
         int cy = unit_float(h.y) < fy ? hy : ly;
         int cz = unit_float(h.z) < fz ? hz : lz;
@@ -269,7 +271,7 @@ GG_API int gg_splat_bin(gg_particles* ps, gg_volume* vol, const SplatUniforms* u
     gg_context* ctx = vol->ctx;
     std::lock_guard<std::recursive_mutex> lock(ctx->mu);
     GG_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
-    SplatArgs a{ps->pos, ps->vel, vol->sums, *u};
+    SplatArgs a{ps->pos, ps->vel, vol->sums, *u, ps->first_index};
     bin_kernel<<<(ps->count + 255u) / 256u, 256, 0, ctx->stream>>>(a);
     return gg::launch_status("splat bin");
 }
@@ -321,6 +323,35 @@ GG_API int gg_volume_read_sums(gg_volume* vol, uint32_t* emission, int32_t* mome
         momentum[3 * i + 2] = (int32_t)rec[6 * i + 4];
         mass[i] = rec[6 * i + 5];
     }
+    return GG_OK;
+}
+
+GG_API int gg_volume_write_sums(gg_volume* vol, const uint32_t* emission, const int32_t* momentum, const uint32_t* mass) {
+    if (!vol || !emission || !momentum || !mass)
+        return gg::fail(GG_ERR_INVALID_ARGUMENT, "gg_volume_write_sums needs a volume and three input arrays.");
+    gg_context* ctx = vol->ctx;
+    std::lock_guard<std::recursive_mutex> lock(ctx->mu);
+    GG_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
+    const uint64_t voxels = (uint64_t)vol->size * vol->size * vol->size;
+    std::vector<uint32_t> rec(voxels * 6u);
+    for (uint64_t i = 0; i < voxels; ++i) {
+        rec[6 * i + 0] = emission[2 * i + 0];
+        rec[6 * i + 1] = emission[2 * i + 1];
+        rec[6 * i + 2] = (uint32_t)momentum[3 * i + 0];
+        rec[6 * i + 3] = (uint32_t)momentum[3 * i + 1];
+        rec[6 * i + 4] = (uint32_t)momentum[3 * i + 2];
+        rec[6 * i + 5] = mass[i];
+    }
+    GG_CUDA(cudaMemcpyAsync(vol->sums, rec.data(), voxels * 24u, cudaMemcpyHostToDevice, ctx->stream), "sums upload");
+    GG_CUDA(cudaStreamSynchronize(ctx->stream), "sums upload");
+    return GG_OK;
+}
+
+GG_API int gg_volume_sums(gg_volume* vol, void** device_words, uint64_t* words) {
+    if (!vol || !device_words || !words)
+        return gg::fail(GG_ERR_INVALID_ARGUMENT, "gg_volume_sums needs a volume and two outputs.");
+    *device_words = vol->sums;
+    *words = (uint64_t)vol->size * vol->size * vol->size * 6u;
     return GG_OK;
 }
 

@@ -190,6 +190,7 @@ class Context:
 
     def __init__(self, device: int = 0, budget_bytes: int = 0):
         self.handle = C.c_void_p()
+        self.device = device
         self._children = weakref.WeakSet()
         check(lib().gg_context_create(device, budget_bytes, C.byref(self.handle)))
 
@@ -269,12 +270,14 @@ def probe_results_to_numpy(res) -> dict:
 class Particles:
     """ParticleSystem (Sim/ParticleSystem.swift) + SimPass (Passes/SimPass.swift)."""
 
-    def __init__(self, ctx: Context, count: int, seed: int = 1, potential: int = T.POTENTIAL_PACZYNSKI_WIITA):
+    def __init__(self, ctx: Context, count: int, seed: int = 1, potential: int = T.POTENTIAL_PACZYNSKI_WIITA,
+                 first_index: int = 0):
         self.ctx = ctx
         self.count = count
         self.seed = seed
+        self.first_index = first_index
         self.handle = C.c_void_p()
-        check(lib().gg_particles_create(ctx.handle, count, seed, potential, C.byref(self.handle)))
+        check(lib().gg_particles_create_shard(ctx.handle, count, first_index, seed, potential, C.byref(self.handle)))
         ctx.adopt(self)
 
     def close(self):
@@ -388,6 +391,12 @@ class Volume:
         ma = np.zeros(n3, np.uint32)
         check(lib().gg_volume_read_sums(self.handle, ptr(em), ptr(mo), ptr(ma)))
         return em, mo, ma
+
+    def write_sums(self, em: np.ndarray, mo: np.ndarray, ma: np.ndarray):
+        em = np.ascontiguousarray(em, np.uint32)
+        mo = np.ascontiguousarray(mo, np.int32)
+        ma = np.ascontiguousarray(ma, np.uint32)
+        check(lib().gg_volume_write_sums(self.handle, ptr(em), ptr(mo), ptr(ma)))
 
     def read(self):
         n3 = self.size ** 3

@@ -97,6 +97,14 @@ GG_API int gg_particles_create(gg_context* ctx, uint32_t count, uint64_t seed, u
                                gg_particles** out);
 GG_API void gg_particles_destroy(gg_particles* ps);
 
+/* A shard of a larger particle system: `count` particles whose global
+ * indices start at first_index. The counter-based hash is keyed on the
+ * global index (sim.metal:7-8, splat.metal:75), so shards on several GPUs
+ * reproduce the unsharded system slot for slot and their splat grids sum to
+ * the unsharded grid exactly. No reference counterpart (one GPU there). */
+GG_API int gg_particles_create_shard(gg_context* ctx, uint32_t count, uint32_t first_index, uint64_t seed,
+                                     uint32_t potential, gg_particles** out);
+
 /* The uniforms the particle kernels run with (ParticleSystem.swift:59-70). */
 GG_API int gg_particles_uniforms(gg_particles* ps, SimUniforms* out);
 
@@ -153,6 +161,19 @@ GG_API int gg_volume_clear(gg_volume* vol);
  * emission u32[2 n^3] (energy, energy*T pairs), momentum i32[3 n^3], mass
  * u32[n^3], voxel index (z n + y) n + x (splat.metal:21-23). */
 GG_API int gg_volume_read_sums(gg_volume* vol, uint32_t* emission, int32_t* momentum, uint32_t* mass);
+
+/* Replace the sums with host arrays in the same layouts, e.g. after summing
+ * the grids of several GPUs' particle shards. */
+GG_API int gg_volume_write_sums(gg_volume* vol, const uint32_t* emission, const int32_t* momentum, const uint32_t* mass);
+
+/* Device address and length (in 32-bit words) of the volume's sums: one
+ * record of six words per voxel (energy, energy*T, momentum x/y/z, mass),
+ * voxel index (z n + y) n + x. Every word is a two's-complement sum, so the
+ * grids of several GPUs' particle shards combine with one element-wise
+ * integer all-reduce (sum) over this buffer, done on the context's stream
+ * (gg_context_stream) between gg_splat_bin and gg_splat_resolve. Valid until
+ * the volume is destroyed. */
+GG_API int gg_volume_sums(gg_volume* vol, void** device_words, uint64_t* words);
 
 /* Copy the resolved textures to host arrays of n^3 half4 (IEEE binary16 bit
  * patterns, x fastest). Replaces Validate.readVolume (Validate.swift:204-230). */

@@ -155,19 +155,20 @@ double o_side_ratio(const double* luminance, int width, int height);
 
 /* FP32 replicas of the particle kernels (sim.metal:6-79 with the sqrt-form
  * powers), bit-exact with the device. SimUniforms fields are passed
- * explicitly. particles: n x 8 words in the Particle layout. */
+ * explicitly. particles: n x 8 words in the Particle layout; slot i is the
+ * particle of global index first_index + i (0 for an unsharded system). */
 void o32_seed(float* particles, uint32_t n, uint32_t seed_lo, uint32_t seed_hi, uint32_t potential,
-              const float* inverse_cdf, uint32_t cdf_count, float temperature_scale);
+              const float* inverse_cdf, uint32_t cdf_count, float temperature_scale, uint32_t first_index);
 void o32_step(float* particles, uint32_t n, uint32_t seed_lo, uint32_t seed_hi, uint32_t potential,
               const float* inverse_cdf, uint32_t cdf_count, float dt, float alpha, float temperature_scale,
-              uint32_t dispatches, int threads);
+              uint32_t dispatches, int threads, uint32_t first_index);
 uint64_t o_fnv1a(const void* bytes, uint64_t count);
 
 /* FP32 replica of the deposit (splat.metal:25-88) into the reference
  * layouts: emission u32[2 n^3], momentum i32[3 n^3], mass u32[n^3]. */
 void o32_deposit(const float* particles, uint32_t count, uint32_t size, float half_extent, float peak_temperature,
                  float emission_scale, uint32_t frame, uint32_t exact, uint32_t seed_lo, uint32_t seed_hi,
-                 uint32_t* emission, int32_t* momentum, uint32_t* mass);
+                 uint32_t* emission, int32_t* momentum, uint32_t* mass, uint32_t first_index);
 
 /* Resolve (splat.metal:93-120) in FP32 with a float blackbody table
  * (count x 3, linearly interpolated); outputs float rgba per voxel. */

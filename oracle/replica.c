@@ -142,21 +142,21 @@ static void step32(uint32_t i, const sim32* u, float* p) {
 }
 
 void o32_seed(float* particles, uint32_t n, uint32_t seed_lo, uint32_t seed_hi, uint32_t potential,
-              const float* cdf, uint32_t cdf_count, float temperature_scale) {
+              const float* cdf, uint32_t cdf_count, float temperature_scale, uint32_t first_index) {
     sim32 u = {seed_lo, seed_hi, potential, cdf_count, cdf, 0.0f, 0.0f, temperature_scale};
-    for (uint32_t i = 0; i < n; ++i) spawn32(i, 0u, &u, 1, particles + 8 * (uint64_t)i);
+    for (uint32_t i = 0; i < n; ++i) spawn32(first_index + i, 0u, &u, 1, particles + 8 * (uint64_t)i);
 }
 
 void o32_step(float* particles, uint32_t n, uint32_t seed_lo, uint32_t seed_hi, uint32_t potential,
               const float* cdf, uint32_t cdf_count, float dt, float alpha, float temperature_scale,
-              uint32_t dispatches, int threads) {
+              uint32_t dispatches, int threads, uint32_t first_index) {
     sim32 u = {seed_lo, seed_hi, potential, cdf_count, cdf, dt, alpha, temperature_scale};
 #ifdef _OPENMP
     if (threads > 0) omp_set_num_threads(threads);
 #endif
 #pragma omp parallel for schedule(static)
     for (int64_t i = 0; i < (int64_t)n; ++i)
-        for (uint32_t d = 0; d < dispatches; ++d) step32((uint32_t)i, &u, particles + 8 * i);
+        for (uint32_t d = 0; d < dispatches; ++d) step32(first_index + (uint32_t)i, &u, particles + 8 * i);
 }
 
 /* Validate.swift:378-387 */
@@ -190,7 +190,7 @@ static void deposit32(uint32_t* em, int32_t* mo, uint32_t* ma, uint32_t index, f
 /* splat.metal:44-88 */
 void o32_deposit(const float* particles, uint32_t count, uint32_t n, float half_extent, float peak_temperature,
                  float emission_scale, uint32_t frame, uint32_t exact, uint32_t seed_lo, uint32_t seed_hi,
-                 uint32_t* em, int32_t* mo, uint32_t* ma) {
+                 uint32_t* em, int32_t* mo, uint32_t* ma, uint32_t first_index) {
     for (uint32_t i = 0; i < count; ++i) {
         const float* p = particles + 8 * (uint64_t)i;
         float pos[3] = {p[0], p[1], p[2]};
@@ -229,7 +229,7 @@ void o32_deposit(const float* particles, uint32_t count, uint32_t n, float half_
             }
         } else {
             uint32_t h[4];
-            pcg(i, frame, seed_lo, seed_hi, h);
+            pcg(first_index + i, frame, seed_lo, seed_hi, h);
             int corner[3];
             for (int a = 0; a < 3; ++a) corner[a] = unitf(h[a]) < frac[a] ? high[a] : low[a];
             uint32_t index = ((uint32_t)corner[2] * n + (uint32_t)corner[1]) * n + (uint32_t)corner[0];

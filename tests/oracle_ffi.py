@@ -150,10 +150,11 @@ def lib() -> C.CDLL:
         "o_lensed_image": (None, [i, i, _dp, i, d, _dp, _dp, P(Settings), d, d, i, _dp, i]),
         "o_luminance": (d, [_dp]),
         "o_side_ratio": (d, [_dp, i, i]),
-        "o32_seed": (None, [_fp, u32, u32, u32, u32, _fp, u32, C.c_float]),
-        "o32_step": (None, [_fp, u32, u32, u32, u32, _fp, u32, C.c_float, C.c_float, C.c_float, u32, i]),
+        "o32_seed": (None, [_fp, u32, u32, u32, u32, _fp, u32, C.c_float, u32]),
+        "o32_step": (None, [_fp, u32, u32, u32, u32, _fp, u32, C.c_float, C.c_float, C.c_float, u32, i, u32]),
         "o_fnv1a": (u64, [C.c_void_p, u64]),
-        "o32_deposit": (None, [_fp, u32, u32, C.c_float, C.c_float, C.c_float, u32, u32, u32, u32, _u32p, _i32p, _u32p]),
+        "o32_deposit": (None, [_fp, u32, u32, C.c_float, C.c_float, C.c_float, u32, u32, u32, u32, _u32p, _i32p, _u32p,
+                                u32]),
         "o32_resolve": (None, [_u32p, _i32p, _u32p, u32, C.c_float, C.c_float, _fp, i, _fp, _fp]),
         "o_pbr_neutral": (None, [_dp, _dp]),
     }
@@ -260,18 +261,19 @@ def sky_table(camera_radius: float, sphere_radius: float, count: int, intervals:
     return out
 
 
-def seed32(n: int, seed: int, potential: int, cdf: np.ndarray, temperature_scale: float) -> np.ndarray:
+def seed32(n: int, seed: int, potential: int, cdf: np.ndarray, temperature_scale: float,
+           first_index: int = 0) -> np.ndarray:
     parts = np.zeros((n, 8), np.float32)
     cdf = np.ascontiguousarray(cdf, np.float32)
-    lib().o32_seed(parts, n, seed & 0xFFFFFFFF, seed >> 32, potential, cdf, len(cdf), temperature_scale)
+    lib().o32_seed(parts, n, seed & 0xFFFFFFFF, seed >> 32, potential, cdf, len(cdf), temperature_scale, first_index)
     return parts
 
 
 def step32(parts: np.ndarray, seed: int, potential: int, cdf: np.ndarray, dt: float, alpha: float,
-           temperature_scale: float, dispatches: int, threads: int = 0) -> None:
+           temperature_scale: float, dispatches: int, threads: int = 0, first_index: int = 0) -> None:
     cdf = np.ascontiguousarray(cdf, np.float32)
     lib().o32_step(parts, len(parts), seed & 0xFFFFFFFF, seed >> 32, potential, cdf, len(cdf), dt, alpha,
-                   temperature_scale, dispatches, threads)
+                   temperature_scale, dispatches, threads, first_index)
 
 
 def fnv1a(buf: np.ndarray) -> int:
@@ -280,13 +282,14 @@ def fnv1a(buf: np.ndarray) -> int:
 
 
 def deposit32(parts: np.ndarray, size: int, frame: int, exact: bool, seed: int, half_extent: float = 30.0,
-              peak_temperature: float = 8000.0, emission_scale: float = 5e-4):
+              peak_temperature: float = 8000.0, emission_scale: float = 5e-4, first_index: int = 0):
     n3 = size ** 3
     em = np.zeros(2 * n3, np.uint32)
     mo = np.zeros(3 * n3, np.int32)
     ma = np.zeros(n3, np.uint32)
     lib().o32_deposit(np.ascontiguousarray(parts, np.float32), len(parts), size, half_extent, peak_temperature,
-                      emission_scale, frame, 1 if exact else 0, seed & 0xFFFFFFFF, seed >> 32, em, mo, ma)
+                      emission_scale, frame, 1 if exact else 0, seed & 0xFFFFFFFF, seed >> 32, em, mo, ma,
+                      first_index)
     return em, mo, ma
 
 
