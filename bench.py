@@ -16,9 +16,14 @@ host output buffers:
          of the step on the device clock (CUDA events), inputs resident;
   e2e    ray steps / wall time from the first submit to the last result in
          host memory (device-to-host copies included).
-The plain per-request baseline serves the same slices one request at a time
-through the plain FP32 image kernel. Latency p50/p99 come from a separate
-open-loop replay of the stream's arrivals at 40 req/s.
+Two per-request baselines serve the same slices one request at a time
+through a thread-per-pixel image kernel: `plain_per_request` with the
+reference's step arithmetic as written (march.metal), and
+`plain_lane_per_request` with this library's plain FP32 step arithmetic,
+which isolates what batching and the persistent kernel add. Latency p50/p99
+come from a separate open-loop replay of the stream's arrivals at 40 req/s.
+`passes` times the particle step and the splat alone against their
+rooflines.
 
 --impl reference times the reference's CPU path, the FP64 oracle's
 integrators (oracle/, a C restatement of gargantua's Swift oracle), on a
@@ -215,6 +220,100 @@ def cpu_sample(slices, seconds: float, threads: int):
     return total_steps / max(elapsed, 1e-9), total_rays, total_steps, elapsed, desc
 
 
+def measured_peaks() -> dict:
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "MEASURED_PEAKS.json")
+    try:
+        with open(path) as fh:
+            return json.load(fh)
+    except OSError:
+        return {}
+
+
+def measure_passes(ctx, g, torch) -> dict:
+    """The particle step and the splat, each timed alone with CUDA events on
+    the library's stream, L2 flushed (a 256 MB write) before every launch.
+
+    sim: the max preset's 4M particles, one dispatch (SIM_SUBSTEPS = 2
+    substeps) reads and writes 32 B per particle: 64 B algorithmic traffic
+    per particle-dispatch, bound by HBM. splat: the default preset's 1M
+    settled particles into 128^3, the shape (brick edge, chunk) picked by
+    gg_splat_autotune; the bin's work is 6 u32 atomic adds per deposit
+    (exact: one per corner), bound by the device's scattered shared-memory
+    atomic rate for the brick deposit (gg_measure_shared_atomic_peak), or
+    the global one for direct atomics (gg_measure_atomic_peak); the resolve
+    reads 24 B, zeroes 24 B and writes 16 B per voxel, bound by HBM."""
+    lib = g.lib()
+    ext = torch.cuda.ExternalStream(lib.gg_context_stream(ctx.handle))
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+
+    def timed(fn, pre=None, iters=20, warm=3):
+        pairs = []
+        for k in range(warm + iters):
+            if pre is not None:
+                pre()
+            with torch.cuda.stream(ext):
+                flush.zero_()
+            e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            e0.record(ext)
+            fn()
+            e1.record(ext)
+            if k >= warm:
+                pairs.append((e0, e1))
+        ext.synchronize()
+        return sum(a.elapsed_time(b) for a, b in pairs) / len(pairs) * 1e-3
+
+    peaks = measured_peaks()
+    hbm = peaks.get("hbm_gbs", 6650.0)
+    hbm_src = "MEASURED_PEAKS.json hbm_gbs (measured)" if "hbm_gbs" in peaks else "fallback 6650 GB/s"
+    out = {}
+
+    big = g.Particles(ctx, 4_000_000, seed=1)
+    big.advance(10, seed_first=True)
+    t = timed(lambda: big.step(1))
+    gbs = 64.0 * big.count / t / 1e9
+    out["sim"] = {"workload": "4M particles (max preset), one dispatch of 2 substeps", "us": t * 1e6,
+                  "value": 2 * big.count / t, "unit": "particle-steps/s",
+                  "roofline": {"bound": "hbm", "achieved": gbs, "peak": hbm, "unit": "GB/s", "frac": gbs / hbm,
+                               "bytes_per_launch": 64 * big.count, "peak_source": hbm_src}}
+    big.close()
+
+    ps = g.Particles(ctx, 1_000_000, seed=1)
+    ps.advance(300, seed_first=True)
+    parts = ps.read()
+    unit = (parts[:, :3] + np.float32(30.0)) / np.float32(60.0)  # splat.metal:52-53, in float32
+    inside = int(np.all((unit >= 0.0) & (unit < 1.0), axis=1).sum())
+    vol = g.Volume(ctx, 128)
+    atom_peak = ctx.atomic_peak_gadds(128 ** 3)
+    shared_peak = ctx.shared_atomic_peak_gadds()
+    for exact in (True, False):
+        edge, chunk, _ = vol.autotune(ps, exact)
+        deposits = inside * (8 if exact else 1)
+        t = timed(lambda: vol.bin(ps, exact), pre=vol.clear)
+        rate = 6.0 * deposits / t / 1e9
+        peak, src = ((shared_peak, "gg_measure_shared_atomic_peak: scattered u32 shared atomics into a 9^3 "
+                                   "six-word tile") if edge else
+                     (atom_peak, "gg_measure_atomic_peak: scattered u32 REDs into a 128^3 six-word grid"))
+        out["splat_bin_exact" if exact else "splat_bin_stochastic"] = {
+            "workload": "1M settled particles (default preset) into 128^3", "us": t * 1e6,
+            "value": deposits / t, "unit": "deposits/s",
+            "shape": {"brick_edge": edge, "chunk": chunk, "chosen_by": "gg_splat_autotune"},
+            "roofline": {"bound": "shared atomics" if edge else "global atomics", "achieved": rate, "peak": peak,
+                         "unit": "G u32 atomic adds/s", "frac": rate / peak, "peak_source": src,
+                         "global_atomic_peak": atom_peak}}
+    vol.bin(ps, True)
+    t = timed(vol.resolve, pre=lambda: vol.bin(ps, True))
+    gbs = 64.0 * 128 ** 3 / t / 1e9
+    out["splat_resolve"] = {"workload": "128^3 resolve + clear", "us": t * 1e6, "value": 128 ** 3 / t,
+                            "unit": "voxels/s",
+                            "roofline": {"bound": "hbm", "achieved": gbs, "peak": hbm, "unit": "GB/s",
+                                         "frac": gbs / hbm, "bytes_per_launch": 64 * 128 ** 3,
+                                         "peak_source": hbm_src}}
+    vol.close()
+    ps.close()
+    del flush
+    return out
+
+
 def setup_world(device: int, world: int):
     import gargantua_b200 as g
 
@@ -247,6 +346,8 @@ def main():
     ap.add_argument("--requests-per-step", type=int, default=32)
     ap.add_argument("--latency-requests", type=int, default=48)
     ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-passes", action="store_true", help="skip the separate sim and splat timings")
+    ap.add_argument("--no-tune", action="store_true", help="serve with the default wave shape")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     args = ap.parse_args()
 
@@ -305,7 +406,18 @@ def main():
     # Weak scaling: every rank serves its own stream (seed 1 + rank).
     stream = make_stream(1 + rank)
     slices = [stream[i * B:(i + 1) * B] for i in range(nslices)]
-    batched = g.Server(ctx, vol, g.types.SERVE_BATCHED)
+    shape = {"chunk_rays": 32, "wave_rays": 4 << 20, "max_waves_in_flight": 2, "chosen_by": "defaults"}
+    if not args.no_tune:
+        # Untimed: the server's wave shape from a sample of other requests
+        # with the same mix (a different stream seed).
+        from gargantua_b200 import autotune
+
+        sample = [spec_of(q) for q in make_stream(1000 + rank)[:16]]
+        tuned = autotune.tune_server(ctx, vol, sample)
+        shape = {k: tuned[k] for k in ("chunk_rays", "wave_rays", "max_waves_in_flight")}
+        shape["chosen_by"] = "gargantua_b200.autotune.tune_server on 16 requests of stream seed 1000"
+    batched = g.Server(ctx, vol, g.types.SERVE_BATCHED, chunk_rays=shape["chunk_rays"], wave_rays=shape["wave_rays"],
+                       max_waves_in_flight=shape["max_waves_in_flight"])
 
     def barrier():
         torch.cuda.synchronize()
@@ -361,10 +473,11 @@ def main():
     value = steps_all / span_max
     e2e = steps_all / wall_max
 
-    # The plain per-request baseline on the same slices.
-    plain = None
-    if not args.no_plain:
-        server_plain = g.Server(ctx, vol, g.types.SERVE_SERIAL_PLAIN)
+    # The per-request baselines on the same slices: the reference's march as
+    # written, and this library's plain FP32 step arithmetic launched per
+    # request (what batching and compensation add over it).
+    def plain_baseline(mode):
+        server_plain = g.Server(ctx, vol, mode)
         serve_slice(server_plain, slices[0], pinned_outputs(slices[0]))
         barrier()
         p_span = p_wall = p_steps = 0.0
@@ -375,18 +488,28 @@ def main():
             p_steps += sum(r.ray_steps for r in results)
         barrier()
         p_span, p_wall, p_steps = max_over_ranks(p_span), max_over_ranks(p_wall), sum_over_ranks(p_steps)
-        plain = {"value": p_steps / p_span, "e2e": p_steps / p_wall, "unit": "ray-steps/s",
-                 "served_over_plain": value / (p_steps / p_span),
-                 "served_over_plain_e2e": e2e / (p_steps / p_wall)}
-        lat_stream = stream[nslices * B:nslices * B + args.latency_requests]
-        if len(lat_stream) >= 8:
-            plain["p50_ms"], plain["p99_ms"] = latency_replay(server_plain, lat_stream)
+        out = {"value": p_steps / p_span, "e2e": p_steps / p_wall, "unit": "ray-steps/s",
+               "served_over_plain": value / (p_steps / p_span),
+               "served_over_plain_e2e": e2e / (p_steps / p_wall)}
+        lat = stream[nslices * B:nslices * B + args.latency_requests]
+        if len(lat) >= 8:
+            out["p50_ms"], out["p99_ms"] = latency_replay(server_plain, lat)
         server_plain.close()
+        return out
+
+    plain = plain_lane = None
+    if not args.no_plain:
+        plain = plain_baseline(g.types.SERVE_SERIAL_PLAIN_AS_WRITTEN)
+        plain["kernel"] = "per-request image kernel, the reference's step arithmetic as written (march.metal)"
+        plain_lane = plain_baseline(g.types.SERVE_SERIAL_PLAIN)
+        plain_lane["kernel"] = "per-request image kernel, this library's plain FP32 step arithmetic"
 
     lat_stream = stream[nslices * B:nslices * B + args.latency_requests]
     p50 = p99 = None
     if len(lat_stream) >= 8:
         p50, p99 = latency_replay(batched, lat_stream)
+
+    passes = measure_passes(ctx, g, torch) if not args.no_passes else None
 
     cpu = None
     if rank == 0 and world == 1:
@@ -411,10 +534,12 @@ def main():
         "config": {"workload": "served mixed request stream (configs: 40 req/s Poisson; 320x180..3840x2160; "
                                "256/4096 steps; spin 0/0.5/0.9; r 40-120; 1M-particle settled disk, 128^3)",
                    "requests_per_step": B, "stream_seed": 1, "precision": "compensated FP32 + FP64 re-integration",
+                   "server_shape": shape,
                    "l2": "inputs larger than L2 (outputs up to 66 MB per request, 8-200 MB per step)"},
         "p50_ms": p50,
         "p99_ms": p99,
         "plain_per_request": plain,
+        "plain_lane_per_request": plain_lane,
         "drift": {"rays": rays_total, "over_budget": drift_over},
         "e2e": {"value": e2e, "unit": "ray-steps/s", "h2d_bytes_per_step": int(B * 64),
                 "d2h_bytes_per_step": int(d2h / max(args.steps, 1))},
@@ -423,6 +548,7 @@ def main():
                      "peak_source": "measured FP32 FMA microbenchmark (gg_measure_fp32_peak) on this GPU",
                      "kernel": "serve_kernel (persistent, work-stealing)"},
         "cpu_baseline": cpu,
+        "passes": passes,
         "clocks": clock_info,
         "gpu_launches": int(launches * 2 + schw_requests * 2),
     }

@@ -59,6 +59,8 @@ SIGNATURES = {
     "gg_particles_create": (i, [vp, u32, u64, u32, P(vp)]),
     "gg_particles_destroy": (None, [vp]),
     "gg_particles_create_shard": (i, [vp, u32, u32, u64, u32, P(vp)]),
+    "gg_particles_seed_profile": (i, [vp, C.c_float, C.c_float]),
+    "gg_particles_profile_table": (i, [vp, f32p, u32]),
     "gg_particles_uniforms": (i, [vp, P(T.SimUniforms)]),
     "gg_particles_seed": (i, [vp]),
     "gg_particles_step": (i, [vp, u32]),
@@ -75,6 +77,8 @@ SIGNATURES = {
     "gg_volume_read_sums": (i, [vp, vp, vp, vp]),
     "gg_volume_write_sums": (i, [vp, vp, vp, vp]),
     "gg_volume_sums": (i, [vp, P(vp), P(u64)]),
+    "gg_volume_splat_shape": (i, [vp, i, u32, u32]),
+    "gg_splat_autotune": (i, [vp, vp, P(T.SplatUniforms), P(u32), P(u32), P(C.c_float)]),
     "gg_volume_read": (i, [vp, vp, vp]),
     "gg_volume_write": (i, [vp, vp, vp]),
     "gg_tables_update": (i, [vp, C.c_float, P(T.MarchUniforms)]),
@@ -82,8 +86,11 @@ SIGNATURES = {
     "gg_targets_create": (i, [vp, u32, u32, P(vp)]),
     "gg_targets_destroy": (None, [vp]),
     "gg_targets_read": (i, [vp, vp, vp, vp, vp]),
+    "gg_targets_write": (i, [vp, vp, vp]),
     "gg_march": (i, [vp, vp, P(T.MarchUniforms), vp, i, P(T.MarchCounters)]),
     "gg_probe": (i, [vp, P(T.MarchUniforms), vp, vp, u32, i]),
+    "gg_capture_boundary": (i, [vp, P(T.MarchUniforms), vp, vp, vp, C.c_double, C.c_double, u32, u32,
+                                P(C.c_double)]),
     "gg_march_stats": (i, [vp, P(u64), P(u64), P(u64)]),
     "gg_march_compensated_noalloc": (i, [vp, vp, P(T.MarchUniforms), vp, P(T.MarchCounters)]),
     "gg_bake_create": (i, [vp, u32, u32, P(vp)]),
@@ -101,6 +108,8 @@ SIGNATURES = {
     "gg_server_wait": (i, [vp, u64, C.c_double, P(T.RequestResult)]),
     "gg_server_totals": (i, [vp, i, P(u64), P(u64), P(u64), P(C.c_double), P(C.c_double)]),
     "gg_measure_fp32_peak": (i, [vp, P(C.c_double)]),
+    "gg_measure_atomic_peak": (i, [vp, u32, P(C.c_double)]),
+    "gg_measure_shared_atomic_peak": (i, [vp, P(C.c_double)]),
 }
 
 

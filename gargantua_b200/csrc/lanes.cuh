@@ -120,9 +120,25 @@ __device__ __forceinline__ double fmaT(double a, double b, double c) { return fm
 __device__ __forceinline__ float rsqrtT(float x) { return rsqrtf(x); }
 __device__ __forceinline__ double rsqrtT(double x) { return rcp(sqrt(x)); }
 
-// x += y; in FP32 the rounding error is carried in e (TwoSum, march.cuh).
-__device__ __forceinline__ void comp_addT(float& x, float& e, float y) { comp_add(x, e, y); }
-__device__ __forceinline__ void comp_addT(double& x, double& e, double y) { x += y; }
+// Square root for lengths that feed only path lengths and sample positions:
+// FP32 from sqrt.approx (relative error below 2^-22), FP64 exact.
+__device__ __forceinline__ float asqrt(float x) {
+    float y;
+    asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ double asqrt(double x) { return sqrt(x); }
+
+// x += y. Compensated FP32 carries the rounding error in e (TwoSum,
+// march.cuh); plain FP32 and FP64 add directly and leave e at zero.
+template <bool Comp> __device__ __forceinline__ void comp_addT(float& x, float& e, float y) {
+    if constexpr (Comp) {
+        comp_add(x, e, y);
+    } else {
+        x += y;
+    }
+}
+template <bool Comp> __device__ __forceinline__ void comp_addT(double& x, double& e, double y) { x += y; }
 
 template <typename R> __device__ __forceinline__ V3<R> v3_of(float3 a) { return v3<R>(R(a.x), R(a.y), R(a.z)); }
 
@@ -196,9 +212,9 @@ template <typename R> __device__ __forceinline__ V3<R> s_direction(const SLane<R
 // prepareRay (Geodesic.h:130-163) into a lane. Returns true when the ray is
 // sky-only; then *sky holds its asymptotic direction.
 template <typename R>
-__device__ __forceinline__ bool s_init(SLane<R>& l, float3 origin, float3 direction, const MarchUniforms& u,
+__device__ __forceinline__ bool s_init(SLane<R>& l, V3<R> origin, V3<R> direction, const MarchUniforms& u,
                                        const SweepTables& t, float3* sky) {
-    PreparedRay<R> p = prepare_ray(v3_of<R>(origin), v3_of<R>(direction), u, t);
+    PreparedRay<R> p = prepare_ray(origin, direction, u, t);
     l.e1 = p.ray.e1;
     l.e2 = p.ray.e2;
     l.energy = p.ray.energy;
@@ -224,18 +240,24 @@ __device__ __forceinline__ bool s_init(SLane<R>& l, float3 origin, float3 direct
     return false;
 }
 
-template <typename R> __device__ __forceinline__ void s_advance(SState<R>& s, SState<R>& c, R h) {
+template <typename R>
+__device__ __forceinline__ bool s_init(SLane<R>& l, float3 origin, float3 direction, const MarchUniforms& u,
+                                       const SweepTables& t, float3* sky) {
+    return s_init(l, v3_of<R>(origin), v3_of<R>(direction), u, t, sky);
+}
+
+template <typename R, bool Comp> __device__ __forceinline__ void s_advance(SState<R>& s, SState<R>& c, R h) {
     SState<R> inc = s_increment(s, h);
-    comp_addT(s.r, c.r, inc.r);
-    comp_addT(s.phi, c.phi, inc.phi);
-    comp_addT(s.vd, c.vd, inc.vd);
-    comp_addT(s.rd, c.rd, inc.rd);
-    comp_addT(s.pd, c.pd, inc.pd);
+    comp_addT<Comp>(s.r, c.r, inc.r);
+    comp_addT<Comp>(s.phi, c.phi, inc.phi);
+    comp_addT<Comp>(s.vd, c.vd, inc.vd);
+    comp_addT<Comp>(s.rd, c.rd, inc.rd);
+    comp_addT<Comp>(s.pd, c.pd, inc.pd);
 }
 
 // One iteration of marchRay's loop (march.metal:65-106). Returns true when
 // the ray ended (captured, escaped, left the sphere or hit the step cap).
-template <typename R>
+template <typename R, bool Comp = true>
 __device__ __forceinline__ bool s_step(SLane<R>& l, const MarchUniforms& u, cudaTextureObject_t em,
                                        cudaTextureObject_t vel, bool gather) {
     const GeodesicSettings& g = u.geodesic;
@@ -243,18 +265,18 @@ __device__ __forceinline__ bool s_step(SLane<R>& l, const MarchUniforms& u, cuda
     R h = ray_step_length(l.previous.z, l.s.r, g);
     const R sphere = R(u.sphereRadius);
     SState<R> before = l.s, before_c = l.c;
-    s_advance(l.s, l.c, h);
+    s_advance<R, Comp>(l.s, l.c, h);
     l.steps += 1u;
     if (u.sphereRadius > 0.0f && l.s.r >= sphere && l.s.rd > R(0) && before.r < sphere) {
         R frac = (sphere - before.r) / (l.s.r - before.r);
         l.s = before;
         l.c = before_c;
-        s_advance(l.s, l.c, h * frac);
+        s_advance<R, Comp>(l.s, l.c, h * frac);
     }
     R sn, cs;
     V3<R> position = s_position(l, &sn, &cs);
     V3<R> d = position - l.previous;
-    float path = (float)gsqrt(dot(d, d));
+    float path = (float)asqrt(dot(d, d));
     l.travelled += path;
     l.min_r = fminf(l.min_r, (float)l.s.r);
     if (l.s.r <= R(g.captureRadius)) {
@@ -383,9 +405,11 @@ template <typename R> __device__ __forceinline__ void k_sin_inverses(R st, R* in
 template <typename R> __device__ __forceinline__ R k_sin2(R st) { return gmax(st * st, R(sizeof(R) == 4 ? 1e-8 : 1e-12)); }
 
 // Hamilton's equations with the off-shell Sigma terms (Kerr.h:63-90), at a
-// polar angle whose sine and cosine are given.
+// polar angle whose sine and cosine are given. Also returns F = 2 Sigma H,
+// the null residual of the state (Kerr.h:44-50), and 1/sin^2.
 template <typename R>
-__device__ __forceinline__ KState<R> k_derivative(const KConst<R>& k, const KState<R>& s, R st, R ct) {
+__device__ __forceinline__ KState<R> k_derivative(const KConst<R>& k, const KState<R>& s, R st, R ct, R* F_out,
+                                                  R* inv_sin2_out) {
     R r = s.r;
     R r2 = r * r;
     R delta = r2 - R(2) * r + k.a2;
@@ -401,6 +425,8 @@ __device__ __forceinline__ KState<R> k_derivative(const KConst<R>& k, const KSta
     R p2d = p * p * inv_delta;
     R F = fmaT(delta, pr2, fmaT(s.pt, s.pt, g - p2d));
     R ham = R(0.5) * F * inv_sigma;
+    *F_out = F;
+    *inv_sin2_out = inv_sin2;
     R dprime = R(2) * r - R(2);
     R fr = fmaT(dprime, pr2, inv_delta * (p2d * dprime - R(4) * r * k.E * p));
     R fth = R(2) * ct * fmaT(k.a2E2, st, -k.L2 * inv_sin2 * inv_sc);
@@ -418,19 +444,64 @@ template <typename R> __device__ __forceinline__ KState<R> k_offset(const KState
                      fmaT(d.pt, w, s.pt)};
 }
 
-// RK4 increment (Kerr.h:92-99); (st0, ct0) are sin and cos of s.th.
+// sin and cos of theta0 + delta from those of theta0, for |delta| <= 0.35:
+// the angle-addition formulas with Taylor polynomials of sin delta (through
+// delta^7, remainder below 2.2e-10) and cos delta (through delta^8,
+// remainder below 8e-12). False (nothing written) for larger |delta|.
+__device__ __forceinline__ bool sincos_shift(float st0, float ct0, float delta, float* st, float* ct) {
+    if (!(fabsf(delta) <= 0.35f)) return false;
+    float d2 = delta * delta;
+    float ps = fmaf(d2, (float)(-1.0 / 5040.0), (float)(1.0 / 120.0));
+    ps = fmaf(d2, ps, (float)(-1.0 / 6.0));
+    float sd = fmaf(delta * d2, ps, delta);
+    float pc = fmaf(d2, (float)(1.0 / 40320.0), (float)(-1.0 / 720.0));
+    pc = fmaf(d2, pc, (float)(1.0 / 24.0));
+    pc = fmaf(d2, pc, -0.5f);
+    float cd = fmaf(d2, pc, 1.0f);
+    *st = fmaf(st0, cd, ct0 * sd);
+    *ct = fmaf(ct0, cd, -(st0 * sd));
+    return true;
+}
+
+// The conserved-quantity gauge of a state, before the division by
+// max(|Q0|, E^2) (Kerr.h:39-50; march.metal:160-163): the larger of
+// |Q - Q0| and |2 Sigma H| / max(r^2, 1).
+template <typename R> __device__ __forceinline__ R k_gauge(const KConst<R>& k, const KState<R>& s, R ct, R F,
+                                                           R inv_sin2, R carter0) {
+    R carter = fmaT(ct * ct, fmaT(k.L2, inv_sin2, -k.a2E2), s.pt * s.pt);
+    return gmax(gabs(carter - carter0), gabs(F) * rcp(gmax(s.r * s.r, R(1))));
+}
+
+// RK4 increment (Kerr.h:92-99); (st0, ct0) are sin and cos of s.th. The
+// first stage's derivative is evaluated at s itself, so it also yields the
+// gauge of s: when `gauged`, *gauge becomes the larger of itself and it.
+// The later stages take sin and cos of their polar angle by rotating
+// (st0, ct0) through the stage's offset, which is small except near the
+// poles; there the full reduction runs.
 template <typename R>
-__device__ __forceinline__ KState<R> k_increment(const KConst<R>& k, const KState<R>& s, R h, R st0, R ct0) {
+__device__ __forceinline__ KState<R> k_increment(const KConst<R>& k, const KState<R>& s, R h, R st0, R ct0,
+                                                 bool gauged, R carter0, R* gauge) {
     KState<R> acc{R(0), R(0), R(0), R(0), R(0)};
     KState<R> x = s;
     R st = st0, ct = ct0;
+    R shift = R(0);
 #pragma unroll 1
     for (int stage = 0; stage < 4; ++stage) {
-        if (stage > 0) fast_sincos(x.th, &st, &ct);
-        KState<R> d = k_derivative(k, x, st, ct);
+        if (stage > 0) {
+            if constexpr (sizeof(R) == 4) {
+                if (!sincos_shift(st0, ct0, shift, &st, &ct)) fast_sincos(x.th, &st, &ct);
+            } else {
+                fast_sincos(x.th, &st, &ct);
+            }
+        }
+        R F, inv_sin2;
+        KState<R> d = k_derivative(k, x, st, ct, &F, &inv_sin2);
+        if (stage == 0 && gauged) *gauge = gmax(*gauge, k_gauge(k, s, ct, F, inv_sin2, carter0));
         R wk = (stage == 0 || stage == 3) ? R(1) : R(2);
         acc = k_offset(acc, d, wk);
-        x = k_offset(s, d, stage < 2 ? R(0.5) * h : h);
+        const R wx = stage < 2 ? R(0.5) * h : h;
+        x = k_offset(s, d, wx);
+        shift = d.th * wx;
     }
     const R w = h * (R(1) / R(6));
     return KState<R>{acc.r * w, acc.th * w, acc.ph * w, acc.pr * w, acc.pt * w};
@@ -441,7 +512,7 @@ template <typename R> struct KLane {
     KConst<R> k;
     R st, ct;  // sin and cos of s.th
     R carter0, scale, capture;
-    float drift;
+    R gauge;  // max of k_gauge over the states after steps 1 .. steps-1
     float3 color;
     float transmittance, travelled, weighted_depth, depth_weight;
     V3<R> previous;
@@ -463,25 +534,36 @@ template <typename R> __device__ __forceinline__ void k_gauges(const KLane<R>& l
     *residual = fmaT(delta, l.s.pr * l.s.pr, fmaT(l.s.pt, l.s.pt, g - p * p * rcp(delta)));
 }
 
+// The ray's drift (march.metal:160-163: the maximum over the states after
+// every step): the steps' gauges so far and that of the final state,
+// divided by max(|Q0|, E^2).
+template <typename R> __device__ __forceinline__ float k_drift(const KLane<R>& l) {
+    if (l.steps == 0u) return 0.0f;
+    R carter, residual;
+    k_gauges(l, &carter, &residual);
+    R last = gmax(gabs(carter - l.carter0), gabs(residual) * rcp(gmax(l.s.r * l.s.r, R(1))));
+    return (float)(gmax(l.gauge, last) / l.scale);
+}
+
 template <typename R> __device__ __forceinline__ V3<R> k_position(const KLane<R>& l) {
     R sp, cp;
     fast_sincos(l.s.ph, &sp, &cp);
-    R radial = gsqrt(fmaT(l.s.r, l.s.r, l.k.a2));
+    R radial = asqrt(fmaT(l.s.r, l.s.r, l.k.a2));
     return v3<R>(radial * l.st * cp, radial * l.st * sp, l.s.r * l.ct);
 }
 
 // kerrLaunch (Kerr.h:110-148) into a lane.
 template <typename R>
-__device__ __forceinline__ void k_init(KLane<R>& l, float3 origin, float3 direction, const MarchUniforms& u) {
+__device__ __forceinline__ void k_init(KLane<R>& l, V3<R> origin, V3<R> direction, const MarchUniforms& u) {
     const R a = R(u.spin);
-    KerrState<R> s0 = kerr_launch(a, v3_of<R>(origin), v3_of<R>(direction));
+    KerrState<R> s0 = kerr_launch(a, origin, direction);
     l.s = KState<R>{s0.r, s0.theta, s0.phi, s0.pr, s0.ptheta};
     l.c = KState<R>{R(0), R(0), R(0), R(0), R(0)};
     l.k = k_const(a, s0.energy, s0.angularMomentum);
     l.carter0 = kerr_carter(a, s0);
     l.scale = gmax(gabs(l.carter0), s0.energy * s0.energy);
     l.capture = kerr_outer_horizon(a) + R(KERR_CAPTURE_MARGIN);
-    l.drift = 0.0f;
+    l.gauge = R(0);
     l.color = make_float3(0.0f, 0.0f, 0.0f);
     l.transmittance = 1.0f;
     l.travelled = l.weighted_depth = l.depth_weight = 0.0f;
@@ -492,8 +574,15 @@ __device__ __forceinline__ void k_init(KLane<R>& l, float3 origin, float3 direct
     l.min_r = (float)l.s.r;
 }
 
-// One iteration of marchRayKerr's loop (march.metal:140-173).
 template <typename R>
+__device__ __forceinline__ void k_init(KLane<R>& l, float3 origin, float3 direction, const MarchUniforms& u) {
+    k_init(l, v3_of<R>(origin), v3_of<R>(direction), u);
+}
+
+// One iteration of marchRayKerr's loop (march.metal:140-173). The drift of
+// the state it starts from is folded in by k_increment (k_drift adds the
+// final state's).
+template <typename R, bool Comp = true>
 __device__ __forceinline__ bool k_step(KLane<R>& l, const MarchUniforms& u, cudaTextureObject_t em,
                                        cudaTextureObject_t vel, bool gather) {
     const GeodesicSettings& g = u.geodesic;
@@ -502,23 +591,18 @@ __device__ __forceinline__ bool k_step(KLane<R>& l, const MarchUniforms& u, cuda
     R above = l.s.r - (l.capture - R(KERR_CAPTURE_MARGIN));
     R pole = gmin(gmax(l.st * R(1.0 / 0.08), R(0.05)), R(1));
     R h = gmin(gmax(gmin(R(g.stepFactor) * l.s.r, R(0.2) * above) * pole, R(0.002)), R(g.stepMax));
-    KState<R> inc = k_increment(l.k, l.s, h, l.st, l.ct);
-    comp_addT(l.s.r, l.c.r, inc.r);
-    comp_addT(l.s.th, l.c.th, inc.th);
-    comp_addT(l.s.ph, l.c.ph, inc.ph);
-    comp_addT(l.s.pr, l.c.pr, inc.pr);
-    comp_addT(l.s.pt, l.c.pt, inc.pt);
+    KState<R> inc = k_increment(l.k, l.s, h, l.st, l.ct, l.steps > 0u, l.carter0, &l.gauge);
+    comp_addT<Comp>(l.s.r, l.c.r, inc.r);
+    comp_addT<Comp>(l.s.th, l.c.th, inc.th);
+    comp_addT<Comp>(l.s.ph, l.c.ph, inc.ph);
+    comp_addT<Comp>(l.s.pr, l.c.pr, inc.pr);
+    comp_addT<Comp>(l.s.pt, l.c.pt, inc.pt);
     l.steps += 1u;
     fast_sincos(l.s.th, &l.st, &l.ct);
     V3<R> position = k_position(l);
     V3<R> d = position - l.previous;
-    float path = (float)gsqrt(dot(d, d));
+    float path = (float)asqrt(dot(d, d));
     l.travelled += path;
-    R carter, residual;
-    k_gauges(l, &carter, &residual);
-    R cd = gabs(carter - l.carter0) / l.scale;
-    R nd = gabs(residual) / (l.scale * gmax(l.s.r * l.s.r, R(1)));
-    l.drift = fmaxf(l.drift, (float)gmax(cd, nd));
     l.min_r = fminf(l.min_r, (float)l.s.r);
     if (l.s.r <= l.capture) {
         l.outcome = RayCaptured;
@@ -545,7 +629,7 @@ template <typename R>
 __device__ __forceinline__ PixelResult k_finish(const KLane<R>& l, const MarchUniforms& u, const float4* blackbody) {
     PixelResult r;
     r.color = l.color;
-    r.drift = l.drift;
+    r.drift = k_drift(l);
     r.steps = l.steps;
     r.outcome = l.outcome;
     r.depth = l.depth_weight > 0.0f ? l.weighted_depth / l.depth_weight : l.travelled;
@@ -585,7 +669,7 @@ template <typename R> __device__ inline RayProbeResult k_probe_result(const KLan
     V3<R> dir = kerr_direction(l.k.a, ks);
     out.position = {(float)pos.x, (float)pos.y, (float)pos.z};
     out.direction = {(float)dir.x, (float)dir.y, (float)dir.z};
-    out.drift = l.drift;
+    out.drift = k_drift(l);
     out.outcome = l.outcome;
     out.steps = l.steps;
     out.energy = (float)l.k.E;
@@ -595,7 +679,8 @@ template <typename R> __device__ inline RayProbeResult k_probe_result(const KLan
 
 // One pixel through the lane path, run to completion: compensated FP32, or
 // the FP64 re-integration with R = double.
-template <typename R> __device__ inline PixelResult shade_pixel_lane(const MarchParams& p, uint32_t px, uint32_t py) {
+template <typename R, bool Comp = true>
+__device__ inline PixelResult shade_pixel_lane(const MarchParams& p, uint32_t px, uint32_t py) {
     const MarchUniforms& u = p.u;
     const bool gather = p.emission != 0;
     float3 dir = camera_direction(u, px, py);
@@ -604,19 +689,24 @@ template <typename R> __device__ inline PixelResult shade_pixel_lane(const March
         KLane<R> l;
         k_init(l, origin, dir, u);
         for (uint32_t k = 0; k <= STEP_CAP_STILL; ++k)
-            if (k_step(l, u, p.emission, p.velocity, gather)) break;
+            if (k_step<R, Comp>(l, u, p.emission, p.velocity, gather)) break;
         return k_finish(l, u, p.blackbody);
     }
     SLane<R> l;
     float3 sky;
     if (s_init(l, origin, dir, u, p.tables, &sky)) return sky_only_result(sky, u, p.blackbody);
     for (uint32_t k = 0; k <= STEP_CAP_STILL; ++k)
-        if (s_step(l, u, p.emission, p.velocity, gather)) break;
+        if (s_step<R, Comp>(l, u, p.emission, p.velocity, gather)) break;
     return s_finish(l, u, p.tables, p.blackbody);
 }
 
 __device__ inline PixelResult shade_pixel_compensated(const MarchParams& p, uint32_t px, uint32_t py) {
-    return shade_pixel_lane<float>(p, px, py);
+    return shade_pixel_lane<float, true>(p, px, py);
+}
+
+// The plain FP32 march: the same lane code with direct adds.
+__device__ inline PixelResult shade_pixel_plain(const MarchParams& p, uint32_t px, uint32_t py) {
+    return shade_pixel_lane<float, false>(p, px, py);
 }
 
 }  // namespace gg

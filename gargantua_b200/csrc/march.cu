@@ -12,8 +12,10 @@
 
 namespace gg {
 
-template <bool Comp>
+// Mode: GG_PRECISION_PLAIN, _COMPENSATED or _PLAIN_AS_WRITTEN.
+template <int Mode>
 __global__ void __launch_bounds__(64) march_image_kernel(MarchParams p) {
+    constexpr bool Comp = Mode == GG_PRECISION_COMPENSATED;
     const uint32_t gx = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t gy = blockIdx.y * blockDim.y + threadIdx.y;
     const uint32_t px = p.u.tileOrigin.x + gx, py = p.u.tileOrigin.y + gy;
@@ -22,7 +24,9 @@ __global__ void __launch_bounds__(64) march_image_kernel(MarchParams p) {
     PixelResult r{};
     r.outcome = RayEscaped;
     if (active) {
-        r = Comp ? shade_pixel_compensated(p, px, py) : shade_pixel<float, false>(p, px, py);
+        if constexpr (Mode == GG_PRECISION_COMPENSATED) r = shade_pixel_compensated(p, px, py);
+        else if constexpr (Mode == GG_PRECISION_PLAIN) r = shade_pixel_plain(p, px, py);
+        else r = shade_pixel<float, false>(p, px, py);
         const uint32_t local = gy * p.target_width + gx;
         write_pixel(p, local, r);
         if (Comp && p.flagged && needs_fp64(p.u, r)) {
@@ -115,42 +119,83 @@ __device__ RayProbeResult probe_one(const MarchParams& p, const RayProbe& q, flo
     return out;
 }
 
-template <bool Comp>
+// One probe through the lane code (the image kernels' arithmetic): plain or
+// compensated FP32, or FP64.
+template <typename R, bool Comp>
+__device__ RayProbeResult probe_lane(const MarchParams& p, const RayProbe& q, float* min_r) {
+    const MarchUniforms& u = p.u;
+    float3 origin = make_float3(q.origin.x, q.origin.y, q.origin.z);
+    float3 dir = make_float3(q.direction.x, q.direction.y, q.direction.z);
+    if (u.spin > 0.0f) {
+        KLane<R> l;
+        k_init(l, origin, dir, u);
+        for (uint32_t k = 0; k <= STEP_CAP_STILL; ++k)
+            if (k_step<R, Comp>(l, u, 0, 0, false)) break;
+        *min_r = l.min_r;
+        return k_probe_result(l);
+    }
+    SLane<R> l;
+    float3 sky;
+    if (s_init(l, origin, dir, u, p.tables, &sky))
+        return probe_one<float, false>(p, q, min_r);  // sky-only: no integration either way
+    for (uint32_t k = 0; k <= STEP_CAP_STILL; ++k)
+        if (s_step<R, Comp>(l, u, 0, 0, false)) break;
+    *min_r = l.min_r;
+    return s_probe_result(l, u, p.tables);
+}
+
+template <int Mode>
 __global__ void __launch_bounds__(64) probe_kernel(MarchParams p, const RayProbe* __restrict__ probes,
                                                    RayProbeResult* __restrict__ results, uint32_t count) {
+    constexpr bool Comp = Mode == GG_PRECISION_COMPENSATED;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= count) return;
     RayProbe q = probes[i];
     float min_r = 0.0f;
     RayProbeResult r;
-    if (Comp) {
-        const MarchUniforms& u = p.u;
-        float3 origin = make_float3(q.origin.x, q.origin.y, q.origin.z);
-        float3 dir = make_float3(q.direction.x, q.direction.y, q.direction.z);
-        if (u.spin > 0.0f) {
-            KLane<float> l;
-            k_init(l, origin, dir, u);
-            for (uint32_t k = 0; k <= STEP_CAP_STILL; ++k)
-                if (k_step(l, u, 0, 0, false)) break;
-            r = k_probe_result(l);
-            min_r = l.min_r;
-        } else {
-            SLane<float> l;
-            float3 sky;
-            if (s_init(l, origin, dir, u, p.tables, &sky)) {
-                r = probe_one<float, false>(p, q, &min_r);  // sky-only: no integration either way
-            } else {
-                for (uint32_t k = 0; k <= STEP_CAP_STILL; ++k)
-                    if (s_step(l, u, 0, 0, false)) break;
-                r = s_probe_result(l, u, p.tables);
-                min_r = l.min_r;
-            }
-        }
-        if (r.drift > u.driftBudget && min_r < 4.0f) r = probe_one<double, false>(p, q, &min_r);
-    } else {
+    if constexpr (Mode == GG_PRECISION_PLAIN_AS_WRITTEN) {
         r = probe_one<float, false>(p, q, &min_r);
+    } else {
+        r = probe_lane<float, Comp>(p, q, &min_r);
+        if (Comp && r.drift > p.u.driftBudget && min_r < 4.0f) r = probe_lane<double, false>(p, q, &min_r);
     }
     results[i] = r;
+}
+
+// One FP64 ray per thread along the family origin -> base + t axis, t at
+// the centres of `count` equal cells of [lo, hi]; its outcome (RayOutcome).
+struct BoundaryArgs {
+    double origin[3], base[3], axis[3];
+    double lo, hi;
+    uint32_t count;
+    uint32_t* outcome;
+};
+
+__global__ void __launch_bounds__(128) boundary_kernel(MarchParams p, BoundaryArgs a) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= a.count) return;
+    const double t = a.lo + (a.hi - a.lo) * ((double)k + 0.5) / (double)a.count;
+    V3<double> o = v3<double>(a.origin[0], a.origin[1], a.origin[2]);
+    V3<double> d = v3<double>(fma(t, a.axis[0], a.base[0]), fma(t, a.axis[1], a.base[1]), fma(t, a.axis[2], a.base[2]));
+    uint32_t outcome;
+    if (p.u.spin > 0.0f) {
+        KLane<double> l;
+        k_init(l, o, d, p.u);
+        for (uint32_t s = 0; s <= STEP_CAP_STILL; ++s)
+            if (k_step<double, false>(l, p.u, 0, 0, false)) break;
+        outcome = l.outcome;
+    } else {
+        SLane<double> l;
+        float3 sky;
+        if (s_init(l, o, d, p.u, p.tables, &sky)) {
+            outcome = RayEscaped;
+        } else {
+            for (uint32_t s = 0; s <= STEP_CAP_STILL; ++s)
+                if (s_step<double, false>(l, p.u, 0, 0, false)) break;
+            outcome = l.outcome;
+        }
+    }
+    a.outcome[k] = outcome;
 }
 
 MarchParams make_params(gg_context* ctx, const gg_volume* vol, const MarchUniforms& u, const gg_sweep* sweep) {
@@ -171,17 +216,23 @@ MarchParams make_params(gg_context* ctx, const gg_volume* vol, const MarchUnifor
 int launch_compensated_image(const MarchParams& p, cudaStream_t stream, int sm_count) {
     dim3 block(MARCH_THREADGROUP_WIDTH, MARCH_THREADGROUP_HEIGHT);
     dim3 grid((p.target_width + block.x - 1) / block.x, (p.target_height + block.y - 1) / block.y);
-    march_image_kernel<true><<<grid, block, 0, stream>>>(p);
+    march_image_kernel<GG_PRECISION_COMPENSATED><<<grid, block, 0, stream>>>(p);
     GG_CHECK(launch_status("compensated march"));
     reintegrate_kernel<<<sm_count, 128, 0, stream>>>(p);
     return launch_status("FP64 re-integration");
 }
 
-int launch_plain_image(const MarchParams& p, cudaStream_t stream) {
+int launch_plain_image(const MarchParams& p, cudaStream_t stream, bool as_written) {
     dim3 block(MARCH_THREADGROUP_WIDTH, MARCH_THREADGROUP_HEIGHT);
     dim3 grid((p.target_width + block.x - 1) / block.x, (p.target_height + block.y - 1) / block.y);
-    march_image_kernel<false><<<grid, block, 0, stream>>>(p);
+    if (as_written) march_image_kernel<GG_PRECISION_PLAIN_AS_WRITTEN><<<grid, block, 0, stream>>>(p);
+    else march_image_kernel<GG_PRECISION_PLAIN><<<grid, block, 0, stream>>>(p);
     return launch_status("plain march");
+}
+
+static bool known_precision(int precision) {
+    return precision == GG_PRECISION_PLAIN || precision == GG_PRECISION_COMPENSATED ||
+           precision == GG_PRECISION_PLAIN_AS_WRITTEN;
 }
 
 // The tables the uniforms enable must exist: sphereRadius > 0 means the
@@ -262,10 +313,22 @@ GG_API int gg_targets_read(gg_targets* t, uint16_t* color, uint16_t* debug, floa
     return GG_OK;
 }
 
+GG_API int gg_targets_write(gg_targets* t, const uint16_t* color, const uint16_t* debug) {
+    if (!t || (!color && !debug)) return gg::fail(GG_ERR_INVALID_ARGUMENT, "gg_targets_write needs targets and pixels.");
+    gg_context* ctx = t->ctx;
+    std::lock_guard<std::recursive_mutex> lock(ctx->mu);
+    GG_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
+    const uint64_t px = (uint64_t)t->width * t->height;
+    if (color) GG_CUDA(cudaMemcpyAsync(t->color, color, px * 8u, cudaMemcpyHostToDevice, ctx->stream), "target upload");
+    if (debug) GG_CUDA(cudaMemcpyAsync(t->debug, debug, px * 8u, cudaMemcpyHostToDevice, ctx->stream), "target upload");
+    GG_CUDA(cudaStreamSynchronize(ctx->stream), "target upload");
+    return GG_OK;
+}
+
 GG_API int gg_march(gg_context* ctx, const gg_volume* vol, const MarchUniforms* u, gg_targets* targets, int precision,
                     MarchCounters* counters) {
     if (!ctx || !targets) return gg::fail(GG_ERR_INVALID_ARGUMENT, "gg_march needs a context and targets.");
-    if (precision != GG_PRECISION_PLAIN && precision != GG_PRECISION_COMPENSATED)
+    if (!gg::known_precision(precision))
         return gg::fail(GG_ERR_INVALID_ARGUMENT, "Unknown precision policy %d.", precision);
     std::lock_guard<std::recursive_mutex> lock(ctx->mu);
     GG_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
@@ -297,11 +360,13 @@ GG_API int gg_march(gg_context* ctx, const gg_volume* vol, const MarchUniforms* 
     dim3 block(MARCH_THREADGROUP_WIDTH, MARCH_THREADGROUP_HEIGHT);
     dim3 grid((targets->width + block.x - 1) / block.x, (targets->height + block.y - 1) / block.y);
     if (comp) {
-        march_image_kernel<true><<<grid, block, 0, ctx->stream>>>(p);
+        march_image_kernel<GG_PRECISION_COMPENSATED><<<grid, block, 0, ctx->stream>>>(p);
         GG_CHECK(gg::launch_status("march"));
         reintegrate_kernel<<<ctx->sm_count, 128, 0, ctx->stream>>>(p);
+    } else if (precision == GG_PRECISION_PLAIN) {
+        march_image_kernel<GG_PRECISION_PLAIN><<<grid, block, 0, ctx->stream>>>(p);
     } else {
-        march_image_kernel<false><<<grid, block, 0, ctx->stream>>>(p);
+        march_image_kernel<GG_PRECISION_PLAIN_AS_WRITTEN><<<grid, block, 0, ctx->stream>>>(p);
     }
     GG_CHECK(gg::launch_status("march"));
     if (counters) {
@@ -325,11 +390,75 @@ GG_API int gg_march_stats(gg_context* ctx, uint64_t* ray_steps, uint64_t* sample
     return GG_OK;
 }
 
+GG_API int gg_capture_boundary(gg_context* ctx, const MarchUniforms* u, const double origin[3], const double base[3],
+                               const double axis[3], double lo, double hi, uint32_t rays_per_round, uint32_t rounds,
+                               double* t_out) {
+    if (!ctx || !origin || !base || !axis || !t_out)
+        return gg::fail(GG_ERR_INVALID_ARGUMENT, "gg_capture_boundary needs a context, three vectors and an output.");
+    if (!(hi > lo) || rays_per_round < 2 || rays_per_round > (1u << 20) || rounds == 0 || rounds > 64)
+        return gg::fail(GG_ERR_INVALID_ARGUMENT,
+                        "gg_capture_boundary needs lo < hi, 2..1048576 rays per round and 1..64 rounds.");
+    std::lock_guard<std::recursive_mutex> lock(ctx->mu);
+    GG_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
+    GG_CHECK(gg::check_uniforms(ctx, u, "gg_capture_boundary"));
+    GG_CHECK(gg::ensure_capacity(ctx, &ctx->probe_buffer, &ctx->probe_capacity, 4ull * rays_per_round,
+                                 "boundary outcomes"));
+    MarchParams p = gg::make_params(ctx, nullptr, *u, &ctx->sweep);
+    BoundaryArgs a;
+    for (int c = 0; c < 3; ++c) {
+        a.origin[c] = origin[c];
+        a.base[c] = base[c];
+        a.axis[c] = axis[c];
+    }
+    a.count = rays_per_round;
+    a.outcome = static_cast<uint32_t*>(ctx->probe_buffer);
+    std::vector<uint32_t> out(rays_per_round);
+    for (uint32_t round = 0; round < rounds; ++round) {
+        a.lo = lo;
+        a.hi = hi;
+        boundary_kernel<<<(rays_per_round + 127u) / 128u, 128, 0, ctx->stream>>>(p, a);
+        GG_CHECK(gg::launch_status("capture boundary"));
+        GG_CUDA(cudaMemcpyAsync(out.data(), a.outcome, 4ull * rays_per_round, cudaMemcpyDeviceToHost, ctx->stream),
+                "boundary readback");
+        GG_CUDA(cudaStreamSynchronize(ctx->stream), "capture boundary");
+        auto t_of = [&](uint32_t k) { return lo + (hi - lo) * ((double)k + 0.5) / (double)rays_per_round; };
+        // The edge follows the last ray whose fate matches the first ray's:
+        // a ray deep on the captured side that a step carries across the
+        // horizon can come out as a spurious escape (the reference's
+        // integrator does the same), so earlier changes are not the edge.
+        const bool first_captured = out[0] == RayCaptured;
+        uint32_t last = rays_per_round;
+        for (uint32_t k = rays_per_round; k-- > 0;)
+            if ((out[k] == RayCaptured) == first_captured) {
+                last = k;
+                break;
+            }
+        const uint32_t k = last + 1;
+        if (k >= rays_per_round) {
+            if (round == 0)
+                return gg::fail(GG_ERR_INVALID_ARGUMENT, "Every ray in [%g, %g] is %s: no capture boundary inside.", lo,
+                                hi, first_captured ? "captured" : "escaping");
+            break;  // the boundary lies between two cells of the last round
+        }
+        // A ray at the edge that orbits until the step cap sits on the
+        // boundary and ends the search (Validate.swift:125-150).
+        if (out[k] == RayExhausted) {
+            *t_out = t_of(k);
+            return GG_OK;
+        }
+        const double nlo = t_of(k - 1), nhi = t_of(k);
+        lo = nlo;
+        hi = nhi;
+    }
+    *t_out = 0.5 * (lo + hi);
+    return GG_OK;
+}
+
 GG_API int gg_probe(gg_context* ctx, const MarchUniforms* u, const RayProbe* probes, RayProbeResult* results,
                     uint32_t count, int precision) {
     if (!ctx || (!probes && count) || (!results && count))
         return gg::fail(GG_ERR_INVALID_ARGUMENT, "gg_probe needs a context and probe arrays.");
-    if (precision != GG_PRECISION_PLAIN && precision != GG_PRECISION_COMPENSATED)
+    if (!gg::known_precision(precision))
         return gg::fail(GG_ERR_INVALID_ARGUMENT, "Unknown precision policy %d.", precision);
     std::lock_guard<std::recursive_mutex> lock(ctx->mu);
     GG_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
@@ -344,8 +473,12 @@ GG_API int gg_probe(gg_context* ctx, const MarchUniforms* u, const RayProbe* pro
     GG_CUDA(cudaMemcpyAsync(d_in, probes, in_bytes, cudaMemcpyHostToDevice, ctx->stream), "probe upload");
     MarchParams p = gg::make_params(ctx, nullptr, *u, &ctx->sweep);
     const unsigned blocks = (count + 63u) / 64u;
-    if (precision == GG_PRECISION_COMPENSATED) probe_kernel<true><<<blocks, 64, 0, ctx->stream>>>(p, d_in, d_out, count);
-    else probe_kernel<false><<<blocks, 64, 0, ctx->stream>>>(p, d_in, d_out, count);
+    if (precision == GG_PRECISION_COMPENSATED)
+        probe_kernel<GG_PRECISION_COMPENSATED><<<blocks, 64, 0, ctx->stream>>>(p, d_in, d_out, count);
+    else if (precision == GG_PRECISION_PLAIN)
+        probe_kernel<GG_PRECISION_PLAIN><<<blocks, 64, 0, ctx->stream>>>(p, d_in, d_out, count);
+    else
+        probe_kernel<GG_PRECISION_PLAIN_AS_WRITTEN><<<blocks, 64, 0, ctx->stream>>>(p, d_in, d_out, count);
     GG_CHECK(gg::launch_status("probe rays"));
     GG_CUDA(cudaMemcpyAsync(results, d_out, out_bytes, cudaMemcpyDeviceToHost, ctx->stream), "probe readback");
     GG_CUDA(cudaStreamSynchronize(ctx->stream), "probe rays");

@@ -86,6 +86,24 @@ static double steady_number_density(double r) {
     return 2.0 * kPi * r * (flux * (r - isco) / std::pow(r, 1.5));
 }
 
+// Inverse CDF of radius for a surface density Sigma ~ r^-p on [R_ISCO,
+// R_DISK_OUTER] (number per dr ~ r^(1-p)), at u = k / (count - 1):
+// r = (r0^q + u (r1^q - r0^q))^(1/q), q = 2 - p (q = 0: r0 (r1/r0)^u).
+void power_law_inverse_cdf(int count, double exponent, double* table) {
+    const double r0 = R_ISCO, r1 = R_DISK_OUTER, q = 2.0 - exponent;
+    for (int k = 0; k < count; ++k) {
+        double u = (double)k / (double)(count - 1);
+        if (std::fabs(q) < 1e-12) {
+            table[k] = r0 * std::pow(r1 / r0, u);
+        } else {
+            double a = std::pow(r0, q), b = std::pow(r1, q);
+            table[k] = std::pow(a + u * (b - a), 1.0 / q);
+        }
+    }
+    table[0] = r0;
+    table[count - 1] = r1;
+}
+
 void radial_inverse_cdf(int count, int resolution, double* table) {
     const double r0 = R_ISCO, r1 = R_DISK_OUTER;
     const double dr = (r1 - r0) / resolution;

@@ -91,6 +91,7 @@ int ensure_capacity(gg_context* ctx, void** ptr, uint64_t* capacity, uint64_t by
 // Host-side table construction (FP64, then rounded), the work
 // ParticleSystem.init does on the host (ParticleSystem.swift:23-47).
 void radial_inverse_cdf(int count, int resolution, double* table);
+void power_law_inverse_cdf(int count, double exponent, double* table);
 void blackbody_table(int count, double tmin, double tmax, double* rgb);
 double disk_shape(double r, double floor);
 
@@ -108,6 +109,8 @@ struct gg_particles {
     gg_context* ctx = nullptr;
     uint32_t count = 0;
     uint32_t first_index = 0;  // global index of slot 0 (shards of a larger system)
+    float* profile_cdf = nullptr;   // optional second seeding table (gg_particles_seed_profile)
+    float profile_fraction = 0.0f;  // share of seeded particles drawn from it
     uint64_t seed = 0;
     uint32_t potential = PotentialPaczynskiWiita;
     float4* pos = nullptr;  // x, y, z, temperature
@@ -127,6 +130,12 @@ struct gg_volume {
     cudaSurfaceObject_t emission_surf = 0;
     cudaSurfaceObject_t velocity_surf = 0;
     uint64_t bytes = 0;
+    // Splat shape per deposit mode ([0] stochastic, [1] exact): brick edge B
+    // (0: direct global atomics) and particles per deposit work item.
+    uint32_t brick_edge[2] = {8u, 8u};
+    uint32_t brick_chunk[2] = {4096u, 2048u};
+    void* brick_scratch = nullptr;  // counts, offsets, cursor, items, sorted slots
+    uint64_t brick_scratch_capacity = 0;
 };
 
 struct gg_targets {

@@ -43,7 +43,7 @@
 namespace gg {
 
 MarchParams make_params(gg_context* ctx, const gg_volume* vol, const MarchUniforms& u, const gg_sweep* sweep);
-int launch_plain_image(const MarchParams& p, cudaStream_t stream);
+int launch_plain_image(const MarchParams& p, cudaStream_t stream, bool as_written);
 
 struct ServeRequest {
     MarchUniforms u;
@@ -405,6 +405,9 @@ static int capture_wave_graph(gg_server* s, WaveSlot& w) {
     return GG_OK;
 }
 
+// The per-request baselines: one request at a time through an image kernel.
+static bool serial(const gg_server* s) { return s->cfg.mode != GG_SERVE_BATCHED; }
+
 static int admit(gg_server* s, const std::shared_ptr<ServedRequest>& r) {
     gg_context* ctx = s->ctx;
     const uint64_t px = r->rays;
@@ -562,7 +565,7 @@ static int run_plain(gg_server* s, ServedRequest& r) {
     p.counters = reinterpret_cast<MarchCounters*>(r.d_stats + 8);
     p.stats = r.d_stats;
     GG_CUDA(cudaEventRecord(s->slots[0].start, s->plain), "plain event");
-    GG_CHECK(launch_plain_image(p, s->plain));
+    GG_CHECK(launch_plain_image(p, s->plain, s->cfg.mode == GG_SERVE_SERIAL_PLAIN_AS_WRITTEN));
     GG_CUDA(cudaEventRecord(s->slots[0].stop, s->plain), "plain event");
     r.next_ray = r.rays;
     s->total_waves += 1;
@@ -581,7 +584,7 @@ static void complete_request(gg_server* s, ServedRequest& r) {
     r.result.ray_steps = r.host_stats[0];
     r.result.samples = r.host_stats[1];
     r.result.fp64_rays = r.host_stats[2];
-    if (s->cfg.mode == GG_SERVE_SERIAL_PLAIN) {
+    if (serial(s)) {
         std::memcpy(&r.result.counters, &r.host_stats[8], sizeof(MarchCounters));
     } else {
         r.result.counters.rays = (uint32_t)r.host_stats[3];
@@ -609,7 +612,7 @@ static void worker_loop(gg_server* s) {
         // Admission in arrival order while the footprint fits.
         bool admitted_any = false;
         while (!s->pending.empty() && s->memory_used + s->pending.front()->footprint <= s->cfg.memory_bytes &&
-               (s->cfg.mode != GG_SERVE_SERIAL_PLAIN || s->admitted.empty())) {
+               (!serial(s) || s->admitted.empty())) {
             auto r = s->pending.front();
             s->pending.pop_front();
             s->memory_used += r->footprint;
@@ -621,7 +624,7 @@ static void worker_loop(gg_server* s) {
         if (status == GG_OK && admitted_any) status = cuda_status(cudaEventRecord(s->built, s->build), "admission");
         // Launch work.
         if (status == GG_OK) {
-            if (s->cfg.mode == GG_SERVE_SERIAL_PLAIN) {
+            if (serial(s)) {
                 for (auto& r : s->admitted)
                     if (r->next_ray < r->rays && status == GG_OK) {
                         lock.unlock();
@@ -697,7 +700,8 @@ GG_API int gg_server_create(gg_context* ctx, const gg_volume* vol, const gg_serv
     s->ctx = ctx;
     s->vol = vol;
     if (config) s->cfg = *config;
-    if (s->cfg.mode != GG_SERVE_BATCHED && s->cfg.mode != GG_SERVE_SERIAL_PLAIN)
+    if (s->cfg.mode != GG_SERVE_BATCHED && s->cfg.mode != GG_SERVE_SERIAL_PLAIN &&
+        s->cfg.mode != GG_SERVE_SERIAL_PLAIN_AS_WRITTEN)
         return gg::fail(GG_ERR_INVALID_ARGUMENT, "Unknown serving mode %d.", s->cfg.mode);
     if (s->cfg.memory_bytes == 0) s->cfg.memory_bytes = (ctx->budget - ctx->used) / 4;
     if (ctx->used + s->cfg.memory_bytes > ctx->budget)
@@ -725,7 +729,7 @@ GG_API int gg_server_create(gg_context* ctx, const gg_volume* vol, const gg_serv
     GG_CUDA(cudaEventCreate(&s->origin), "server events");
     GG_CUDA(cudaEventRecord(s->built, s->build), "server events");
     GG_CUDA(cudaEventRecord(s->origin, s->build), "server events");
-    const int nslots = s->cfg.mode == GG_SERVE_SERIAL_PLAIN ? 1 : (int)s->cfg.max_waves_in_flight;
+    const int nslots = serial(s.get()) ? 1 : (int)s->cfg.max_waves_in_flight;
     s->slots.resize(nslots);
     for (auto& w : s->slots) {
         GG_CUDA(cudaStreamCreateWithFlags(&w.stream, cudaStreamNonBlocking), "wave stream");
@@ -736,7 +740,7 @@ GG_API int gg_server_create(gg_context* ctx, const gg_volume* vol, const gg_serv
         GG_CUDA(cudaEventCreate(&w.fp64_done), "wave events");
         GG_CUDA(cudaEventCreate(&w.start), "wave events");
         GG_CUDA(cudaEventCreate(&w.stop), "wave events");
-        if (s->cfg.mode == GG_SERVE_SERIAL_PLAIN) continue;
+        if (serial(s.get())) continue;
         GG_CHECK(gg::device_alloc(ctx, s->slot_bytes, (void**)&w.device, "wave descriptors"));
         GG_CUDA(cudaHostAlloc((void**)&w.host, gg::slot_offset_flagged(s.get()), cudaHostAllocDefault), "wave staging");
         w.args.header = reinterpret_cast<gg::WaveHeader*>(w.device);

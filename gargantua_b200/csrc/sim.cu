@@ -27,6 +27,8 @@ struct SimArgs {
     const float* __restrict__ inverse_cdf;
     SimUniforms u;
     uint32_t first_index;  // global index of slot 0: the hash is keyed on global indices
+    const float* __restrict__ profile_cdf;  // second seeding table, or null
+    float profile_fraction;                 // share of seeds drawn from it
 };
 
 // Unnormalized thin-disk profile (Common.h:49-53) with the powers as square
@@ -40,7 +42,9 @@ __device__ __forceinline__ float disk_shape_f(float r) {
 __device__ __forceinline__ float len3(float x, float y, float z) { return sqrtf(x * x + y * y + z * z); }
 
 // spawn (sim.metal:6-34): event 0 seeds from the steady profile, later
-// events respawn into the feeding annulus.
+// events respawn into the feeding annulus. With a second seeding table
+// (gg_particles_seed_profile), a seed whose spare hash word h1.z falls below
+// the profile's share reads its radius from that table instead.
 __device__ void spawn(uint32_t index, uint32_t event, const SimArgs& a, bool from_disk, float4& p, float4& v) {
     const SimUniforms& u = a.u;
     uint4 h0 = pcg4d(make_uint4(index, event, u.seed.x, u.seed.y));
@@ -49,10 +53,12 @@ __device__ void spawn(uint32_t index, uint32_t event, const SimArgs& a, bool fro
     float u4 = unit_float(h1.x), u5 = unit_float(h1.y);
     float r;
     if (from_disk) {
+        const float* table =
+            (a.profile_cdf && unit_float(h1.z) < a.profile_fraction) ? a.profile_cdf : a.inverse_cdf;
         float position = u0 * (float)(u.inverseCdfCount - 1u);
         uint32_t k = (uint32_t)position;
         if (k > u.inverseCdfCount - 2u) k = u.inverseCdfCount - 2u;
-        float lo = __ldg(a.inverse_cdf + k), hi = __ldg(a.inverse_cdf + k + 1u);
+        float lo = __ldg(table + k), hi = __ldg(table + k + 1u);
         r = lo + (hi - lo) * (position - (float)k);
     } else {
         float inner = R_FEED_INNER * R_FEED_INNER;
@@ -157,6 +163,8 @@ static SimArgs sim_args(gg_particles* ps) {
     a.inverse_cdf = ps->inverse_cdf;
     a.u = ps->uniforms;
     a.first_index = ps->first_index;
+    a.profile_cdf = ps->profile_cdf;
+    a.profile_fraction = ps->profile_fraction;
     return a;
 }
 
@@ -234,6 +242,7 @@ GG_API void gg_particles_destroy(gg_particles* ps) {
     gg::device_free(ctx, ps->pos, (uint64_t)ps->count * 16u);
     gg::device_free(ctx, ps->vel, (uint64_t)ps->count * 16u);
     gg::device_free(ctx, ps->inverse_cdf, INVERSE_CDF_COUNT * sizeof(float));
+    gg::device_free(ctx, ps->profile_cdf, INVERSE_CDF_COUNT * sizeof(float));
     delete ps;
 }
 
@@ -322,6 +331,40 @@ GG_API int gg_particles_checksum(gg_particles* ps, uint64_t* out) {
         hash *= 0x100000001b3ULL;
     }
     *out = hash;
+    return GG_OK;
+}
+
+GG_API int gg_particles_seed_profile(gg_particles* ps, float fraction, float exponent) {
+    GG_CHECK(check_particles(ps, "gg_particles_seed_profile"));
+    if (!(fraction >= 0.0f && fraction <= 1.0f) || !(exponent >= 0.0f && exponent <= 8.0f))
+        return gg::fail(GG_ERR_INVALID_ARGUMENT, "Seed profile needs a share in [0, 1] and an exponent in [0, 8].");
+    gg_context* ctx = ps->ctx;
+    std::lock_guard<std::recursive_mutex> lock(ctx->mu);
+    GG_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
+    if (!ps->profile_cdf)
+        GG_CHECK(gg::device_alloc(ctx, INVERSE_CDF_COUNT * sizeof(float), (void**)&ps->profile_cdf, "profile table"));
+    std::vector<double> table(INVERSE_CDF_COUNT);
+    gg::power_law_inverse_cdf(INVERSE_CDF_COUNT, (double)exponent, table.data());
+    std::vector<float> tf(table.begin(), table.end());
+    GG_CUDA(cudaMemcpyAsync(ps->profile_cdf, tf.data(), tf.size() * sizeof(float), cudaMemcpyHostToDevice,
+                            ctx->stream),
+            "profile table upload");
+    GG_CUDA(cudaStreamSynchronize(ctx->stream), "profile table upload");
+    ps->profile_fraction = fraction;
+    return GG_OK;
+}
+
+GG_API int gg_particles_profile_table(gg_particles* ps, float* out, uint32_t count) {
+    GG_CHECK(check_particles(ps, "gg_particles_profile_table"));
+    if (!out || count != INVERSE_CDF_COUNT)
+        return gg::fail(GG_ERR_INVALID_ARGUMENT, "gg_particles_profile_table needs %u floats.", INVERSE_CDF_COUNT);
+    if (!ps->profile_cdf) return gg::fail(GG_ERR_INVALID_ARGUMENT, "No seed profile was set.");
+    gg_context* ctx = ps->ctx;
+    std::lock_guard<std::recursive_mutex> lock(ctx->mu);
+    GG_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
+    GG_CUDA(cudaMemcpyAsync(out, ps->profile_cdf, count * sizeof(float), cudaMemcpyDeviceToHost, ctx->stream),
+            "table readback");
+    GG_CUDA(cudaStreamSynchronize(ctx->stream), "table readback");
     return GG_OK;
 }
 

@@ -32,71 +32,272 @@ struct SplatArgs {
     uint32_t first_index;  // global index of slot 0, for the stochastic pick
 };
 
-// One corner's six fixed-point atomics (splat.metal:25-37).
-__device__ __forceinline__ void deposit(uint32_t* sums, uint32_t index, float weight, float energy, float relative,
-                                        float vx, float vy, float vz) {
-    uint32_t fe = (uint32_t)(energy * weight * ENERGY_FIXED + 0.5f);
-    uint32_t fet = (uint32_t)(energy * relative * weight * ENERGY_T_FIXED + 0.5f);
-    float ms = weight * MOMENTUM_FIXED;
-    int32_t mx = (int32_t)rintf(vx * ms), my = (int32_t)rintf(vy * ms), mz = (int32_t)rintf(vz * ms);
-    uint32_t fm = (uint32_t)(weight * MASS_FIXED + 0.5f);
-    uint32_t* rec = sums + 6u * index;
-    atomicAdd(rec + 0, fe);
-    atomicAdd(rec + 1, fet);
-    atomicAdd(rec + 2, (uint32_t)mx);
-    atomicAdd(rec + 3, (uint32_t)my);
-    atomicAdd(rec + 4, (uint32_t)mz);
-    atomicAdd(rec + 5, fm);
-}
+// A particle's cloud-in-cell footprint (splat.metal:44-70): positions mapped
+// to voxel-centre space of a cube of half extent u.halfExtent, the low and
+// high corner of each axis, the fractional offsets, and the energy terms.
+struct Footprint {
+    int lx, ly, lz, hx, hy, hz;
+    float fx, fy, fz, energy, relative;
+};
 
-// splatParticles (splat.metal:44-88): positions mapped to voxel-centre
-// space of a cube of half extent u.halfExtent; exact mode deposits all eight
-// corners with trilinear weights, stochastic mode one corner drawn with
-// those weights as probabilities from pcg4d(i, frame, seed).
-__global__ void __launch_bounds__(256) bin_kernel(SplatArgs a) {
-    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    const SplatUniforms& u = a.u;
-    if (i >= u.particleCount) return;
-    float4 p = a.pos[i];
-    const uint32_t gi = a.first_index + i;
+__device__ __forceinline__ bool footprint(float4 p, const SplatUniforms& u, Footprint& f) {
     float ux = (p.x + u.halfExtent) / (2.0f * u.halfExtent);
     float uy = (p.y + u.halfExtent) / (2.0f * u.halfExtent);
     float uz = (p.z + u.halfExtent) / (2.0f * u.halfExtent);
-    if (ux < 0.0f || uy < 0.0f || uz < 0.0f || ux >= 1.0f || uy >= 1.0f || uz >= 1.0f) return;
-    float4 v = a.vel[i];
-    float relative = p.w / u.peakTemperature;
-    float energy = relative * relative * relative * relative * u.emissionScale;
+    if (ux < 0.0f || uy < 0.0f || uz < 0.0f || ux >= 1.0f || uy >= 1.0f || uz >= 1.0f) return false;
+    f.relative = p.w / u.peakTemperature;
+    f.energy = f.relative * f.relative * f.relative * f.relative * u.emissionScale;
     const int n = (int)u.volumeSize;
     float gx = ux * (float)n - 0.5f, gy = uy * (float)n - 0.5f, gz = uz * (float)n - 0.5f;
     float bx = floorf(gx), by = floorf(gy), bz = floorf(gz);
-    float fx = gx - bx, fy = gy - by, fz = gz - bz;
+    f.fx = gx - bx;
+    f.fy = gy - by;
+    f.fz = gz - bz;
     int lx = (int)bx, ly = (int)by, lz = (int)bz;
-    int hx = min(lx + 1, n - 1), hy = min(ly + 1, n - 1), hz = min(lz + 1, n - 1);
-    lx = max(lx, 0);
-    ly = max(ly, 0);
-    lz = max(lz, 0);
+    f.hx = min(lx + 1, n - 1);
+    f.hy = min(ly + 1, n - 1);
+    f.hz = min(lz + 1, n - 1);
+    f.lx = max(lx, 0);
+    f.ly = max(ly, 0);
+    f.lz = max(lz, 0);
+    return true;
+}
+
+// One corner's six fixed-point values (splat.metal:25-37): energy, energy *
+// T, momentum x/y/z, mass.
+struct Deposit {
+    uint32_t w[6];
+};
+
+__device__ __forceinline__ Deposit deposit_values(float weight, float energy, float relative, float vx, float vy,
+                                                  float vz) {
+    Deposit d;
+    d.w[0] = (uint32_t)(energy * weight * ENERGY_FIXED + 0.5f);
+    d.w[1] = (uint32_t)(energy * relative * weight * ENERGY_T_FIXED + 0.5f);
+    float ms = weight * MOMENTUM_FIXED;
+    d.w[2] = (uint32_t)(int32_t)rintf(vx * ms);
+    d.w[3] = (uint32_t)(int32_t)rintf(vy * ms);
+    d.w[4] = (uint32_t)(int32_t)rintf(vz * ms);
+    d.w[5] = (uint32_t)(weight * MASS_FIXED + 0.5f);
+    return d;
+}
+
+// The corners a particle deposits into: exact mode all eight with trilinear
+// weights (w <= 0 skipped), stochastic mode one corner drawn with those
+// weights as probabilities from pcg4d(global index, frame, seed), weight 1.
+// Calls emit(x, y, z, weight) per corner.
+template <typename Emit>
+__device__ __forceinline__ void for_each_corner(const Footprint& f, const SplatUniforms& u, uint32_t global_index,
+                                                Emit emit) {
     if (u.exactDeposit != 0u) {
 #pragma unroll
         for (uint32_t c = 0; c < CIC_CORNERS; ++c) {
             bool bxs = (c & 1u) != 0u, bys = (c & 2u) != 0u, bzs = (c & 4u) != 0u;
-            float wx = bxs ? fx : 1.0f - fx;
-            float wy = bys ? fy : 1.0f - fy;
-            float wz = bzs ? fz : 1.0f - fz;
+            float wx = bxs ? f.fx : 1.0f - f.fx;
+            float wy = bys ? f.fy : 1.0f - f.fy;
+            float wz = bzs ? f.fz : 1.0f - f.fz;
             float w = wx * wy * wz;
             if (w <= 0.0f) continue;
-            uint32_t index = ((uint32_t)(bzs ? hz : lz) * (uint32_t)n + (uint32_t)(bys ? hy : ly)) * (uint32_t)n +
-                             (uint32_t)(bxs ? hx : lx);
-            deposit(a.sums, index, w, energy, relative, v.x, v.y, v.z);
+            emit(bxs ? f.hx : f.lx, bys ? f.hy : f.ly, bzs ? f.hz : f.lz, w);
         }
     } else {
-        uint4 h = pcg4d(make_uint4(gi, u.frame, u.seed.x, u.seed.y));
-        int cx = unit_float(h.x) < fx ? hx : lx;
-        int cy = unit_float(h.y) < fy ? hy : ly;
-        int cz = unit_float(h.z) < fz ? hz : lz;
-        uint32_t index = ((uint32_t)cz * (uint32_t)n + (uint32_t)cy) * (uint32_t)n + (uint32_t)cx;
-        deposit(a.sums, index, 1.0f, energy, relative, v.x, v.y, v.z);
+        uint4 h = pcg4d(make_uint4(global_index, u.frame, u.seed.x, u.seed.y));
+        emit(unit_float(h.x) < f.fx ? f.hx : f.lx, unit_float(h.y) < f.fy ? f.hy : f.ly,
+             unit_float(h.z) < f.fz ? f.hz : f.lz, 1.0f);
     }
 }
+
+// splatParticles (splat.metal:44-88), one thread per particle, six global
+// atomics per corner straight into the sums.
+__global__ void __launch_bounds__(256) bin_kernel(SplatArgs a) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const SplatUniforms& u = a.u;
+    if (i >= u.particleCount) return;
+    Footprint f;
+    if (!footprint(a.pos[i], u, f)) return;
+    const float4 v = a.vel[i];
+    const uint32_t n = u.volumeSize;
+    for_each_corner(f, u, a.first_index + i, [&](int x, int y, int z, float w) {
+        Deposit d = deposit_values(w, f.energy, f.relative, v.x, v.y, v.z);
+        uint32_t* rec = a.sums + 6u * (((uint32_t)z * n + (uint32_t)y) * n + (uint32_t)x);
+#pragma unroll
+        for (int k = 0; k < 6; ++k) atomicAdd(rec + k, d.w[k]);
+    });
+}
+
+// ---------------------------------------------------------------------------
+// Brick-privatised splat. The grid is cut into bricks of B^3 voxels; a
+// particle belongs to the brick holding its low corner, so its eight corners
+// fall in that brick's (B+1)^3 tile. Four launches:
+//   count    per-block shared histogram of particles per brick, summed into
+//            global counts;
+//   scan     one block: brick offsets and work items (ceil(count / chunk)
+//            particles-chunks per brick);
+//   scatter  the same histogram again, each block reserving its range of
+//            every brick with one atomic, then particle indices written into
+//            brick order;
+//   deposit  one block per work item: the tile's six-word records zeroed in
+//            shared memory, the chunk's particles deposited there with
+//            shared atomics, the non-zero words added to the sums with one
+//            global atomic each.
+// Integer sums do not depend on the order of the adds, so the grid equals
+// the direct kernel's bit for bit.
+
+constexpr uint32_t kBrickBlock = 256;
+constexpr uint32_t kBrickParticlesPerBlock = 8192;  // count/scatter range of one block
+constexpr uint32_t kMaxBricks = 32768;               // histogram of 128 KB shared memory
+
+struct BrickArgs {
+    const float4* __restrict__ pos;
+    const float4* __restrict__ vel;
+    uint32_t* __restrict__ sums;
+    SplatUniforms u;
+    uint32_t first_index;
+    uint32_t edge;       // B
+    uint32_t per_axis;   // ceil(n / B)
+    uint32_t bricks;     // per_axis^3
+    uint32_t chunk;      // particles per deposit work item
+    uint32_t* counts;    // [bricks]
+    uint32_t* offsets;   // [bricks + 1], exclusive scan of counts
+    uint32_t* cursor;    // [bricks], reservation cursor
+    uint32_t* items;     // [bricks + 1], exclusive scan of ceil(count / chunk)
+    uint32_t* sorted;    // [particleCount], particle slots in brick order
+};
+
+__device__ __forceinline__ uint32_t brick_of(const Footprint& f, const BrickArgs& a) {
+    return ((uint32_t)f.lz / a.edge * a.per_axis + (uint32_t)f.ly / a.edge) * a.per_axis + (uint32_t)f.lx / a.edge;
+}
+
+__global__ void __launch_bounds__(kBrickBlock) brick_count_kernel(BrickArgs a) {
+    extern __shared__ uint32_t hist[];
+    for (uint32_t b = threadIdx.x; b < a.bricks; b += blockDim.x) hist[b] = 0u;
+    __syncthreads();
+    const uint32_t begin = blockIdx.x * kBrickParticlesPerBlock;
+    const uint32_t end = min(begin + kBrickParticlesPerBlock, a.u.particleCount);
+    for (uint32_t i = begin + threadIdx.x; i < end; i += blockDim.x) {
+        Footprint f;
+        if (footprint(a.pos[i], a.u, f)) atomicAdd(&hist[brick_of(f, a)], 1u);
+    }
+    __syncthreads();
+    for (uint32_t b = threadIdx.x; b < a.bricks; b += blockDim.x)
+        if (hist[b]) atomicAdd(&a.counts[b], hist[b]);
+}
+
+// One block of 1024 threads: each thread scans a contiguous run of bricks.
+__global__ void __launch_bounds__(1024) brick_scan_kernel(BrickArgs a) {
+    __shared__ uint32_t part_p[1024], part_i[1024];
+    const uint32_t per = (a.bricks + blockDim.x - 1) / blockDim.x;
+    const uint32_t b0 = threadIdx.x * per, b1 = min(b0 + per, a.bricks);
+    uint32_t sp = 0, si = 0;
+    for (uint32_t b = b0; b < b1; ++b) {
+        sp += a.counts[b];
+        si += (a.counts[b] + a.chunk - 1u) / a.chunk;
+    }
+    part_p[threadIdx.x] = sp;
+    part_i[threadIdx.x] = si;
+    __syncthreads();
+    // Hillis-Steele inclusive scan of the per-thread totals.
+    for (uint32_t off = 1; off < blockDim.x; off <<= 1) {
+        uint32_t vp = threadIdx.x >= off ? part_p[threadIdx.x - off] : 0u;
+        uint32_t vi = threadIdx.x >= off ? part_i[threadIdx.x - off] : 0u;
+        __syncthreads();
+        part_p[threadIdx.x] += vp;
+        part_i[threadIdx.x] += vi;
+        __syncthreads();
+    }
+    uint32_t op = threadIdx.x ? part_p[threadIdx.x - 1] : 0u;
+    uint32_t oi = threadIdx.x ? part_i[threadIdx.x - 1] : 0u;
+    for (uint32_t b = b0; b < b1; ++b) {
+        a.offsets[b] = op;
+        a.cursor[b] = op;
+        a.items[b] = oi;
+        op += a.counts[b];
+        oi += (a.counts[b] + a.chunk - 1u) / a.chunk;
+    }
+    if (threadIdx.x == blockDim.x - 1) {
+        a.offsets[a.bricks] = part_p[blockDim.x - 1];
+        a.items[a.bricks] = part_i[blockDim.x - 1];
+    }
+}
+
+__global__ void __launch_bounds__(kBrickBlock) brick_scatter_kernel(BrickArgs a) {
+    extern __shared__ uint32_t hist[];
+    for (uint32_t b = threadIdx.x; b < a.bricks; b += blockDim.x) hist[b] = 0u;
+    __syncthreads();
+    const uint32_t begin = blockIdx.x * kBrickParticlesPerBlock;
+    const uint32_t end = min(begin + kBrickParticlesPerBlock, a.u.particleCount);
+    for (uint32_t i = begin + threadIdx.x; i < end; i += blockDim.x) {
+        Footprint f;
+        if (footprint(a.pos[i], a.u, f)) atomicAdd(&hist[brick_of(f, a)], 1u);
+    }
+    __syncthreads();
+    // This block's range of every brick it touches, then a shared cursor.
+    for (uint32_t b = threadIdx.x; b < a.bricks; b += blockDim.x)
+        if (hist[b]) hist[b] = atomicAdd(&a.cursor[b], hist[b]);
+    __syncthreads();
+    for (uint32_t i = begin + threadIdx.x; i < end; i += blockDim.x) {
+        Footprint f;
+        if (!footprint(a.pos[i], a.u, f)) continue;
+        const uint32_t slot = atomicAdd(&hist[brick_of(f, a)], 1u);
+        if (slot < a.u.particleCount) a.sorted[slot] = i;  // always: the count pass saw the same particles
+    }
+}
+
+// Work item -> brick: the last b with items[b] <= item (items is
+// non-decreasing, items[0] = 0).
+__device__ __forceinline__ uint32_t item_brick(const uint32_t* items, uint32_t bricks, uint32_t item) {
+    uint32_t lo = 0, hi = bricks;  // invariant: items[lo] <= item < items[hi]
+    while (hi - lo > 1u) {
+        uint32_t mid = (lo + hi) >> 1;
+        if (items[mid] <= item) lo = mid;
+        else hi = mid;
+    }
+    return lo;
+}
+
+template <uint32_t B>
+__global__ void __launch_bounds__(kBrickBlock) brick_deposit_kernel(BrickArgs a) {
+    constexpr uint32_t T = B + 1;
+    constexpr uint32_t kWords = T * T * T * 6u;
+    extern __shared__ uint32_t tile[];
+    const uint32_t item = blockIdx.x;
+    if (item >= a.items[a.bricks]) return;
+    const uint32_t b = item_brick(a.items, a.bricks, item);
+    const uint32_t j = item - a.items[b];
+    const uint32_t begin = a.offsets[b] + j * a.chunk;
+    const uint32_t end = min(begin + a.chunk, a.offsets[b + 1]);
+    const uint32_t bx = b % a.per_axis, by = (b / a.per_axis) % a.per_axis, bz = b / (a.per_axis * a.per_axis);
+    const int ox = (int)(bx * B), oy = (int)(by * B), oz = (int)(bz * B);
+    for (uint32_t w = threadIdx.x; w < kWords; w += blockDim.x) tile[w] = 0u;
+    __syncthreads();
+    for (uint32_t k = begin + threadIdx.x; k < end; k += blockDim.x) {
+        const uint32_t i = a.sorted[k];
+        Footprint f;
+        // Always inside and in this brick (the count pass put it here); the
+        // test keeps every tile index in bounds regardless.
+        if (!footprint(a.pos[i], a.u, f)) continue;
+        if ((uint32_t)(f.lx - ox) >= B || (uint32_t)(f.ly - oy) >= B || (uint32_t)(f.lz - oz) >= B) continue;
+        const float4 v = a.vel[i];
+        for_each_corner(f, a.u, a.first_index + i, [&](int x, int y, int z, float w) {
+            Deposit d = deposit_values(w, f.energy, f.relative, v.x, v.y, v.z);
+            uint32_t* rec = tile + 6u * (((uint32_t)(z - oz) * T + (uint32_t)(y - oy)) * T + (uint32_t)(x - ox));
+#pragma unroll
+            for (int c = 0; c < 6; ++c) atomicAdd(rec + c, d.w[c]);
+        });
+    }
+    __syncthreads();
+    const uint32_t n = a.u.volumeSize;
+    for (uint32_t w = threadIdx.x; w < kWords; w += blockDim.x) {
+        const uint32_t val = tile[w];
+        if (!val) continue;
+        const uint32_t cell = w / 6u, c = w - cell * 6u;
+        const uint32_t tx = cell % T, ty = (cell / T) % T, tz = cell / (T * T);
+        const uint32_t x = (uint32_t)ox + tx, y = (uint32_t)oy + ty, z = (uint32_t)oz + tz;
+        if (x < n && y < n && z < n) atomicAdd(a.sums + 6u * ((z * n + y) * n + x) + c, val);
+    }
+}
+
+template <uint32_t B> constexpr uint32_t tile_bytes() { return (B + 1) * (B + 1) * (B + 1) * 6u * 4u; }
 
 struct ResolveArgs {
     uint32_t* __restrict__ sums;
@@ -171,6 +372,93 @@ __global__ void clear_kernel(uint4* sums, uint64_t count16) {
 }  // namespace gg
 
 using namespace gg;
+
+static uint32_t bricks_per_axis(uint32_t size, uint32_t edge) { return (size + edge - 1u) / edge; }
+
+// Shapes gg_splat_bin runs: edge 0 (direct), or 4, 8, 16 with a positive
+// chunk and at most kMaxBricks bricks.
+static int check_shape(const gg_volume* vol, uint32_t edge, uint32_t chunk) {
+    if (edge == 0u) return GG_OK;
+    if (edge != 4u && edge != 8u && edge != 16u)
+        return gg::fail(GG_ERR_INVALID_ARGUMENT, "Brick edge %u is not 0, 4, 8 or 16.", edge);
+    if (chunk == 0u || chunk > (1u << 24))
+        return gg::fail(GG_ERR_INVALID_ARGUMENT, "Chunk %u is outside 1..16777216 particles.", chunk);
+    const uint64_t per = bricks_per_axis(vol->size, edge);
+    if (per * per * per > kMaxBricks)
+        return gg::fail(GG_ERR_INVALID_ARGUMENT, "A %u^3 volume in %u^3 bricks makes %llu bricks, over %u.", vol->size,
+                        edge, (unsigned long long)(per * per * per), kMaxBricks);
+    return GG_OK;
+}
+
+// Opt the kernels that need more than 48 KB of dynamic shared memory in,
+// once per device.
+static int allow_shared(const void* kernel, int bytes, int device, int slot) {
+    static std::mutex mu;
+    static int done[64][4] = {};
+    if (bytes <= 48 * 1024 || device >= 64) return GG_OK;
+    std::lock_guard<std::mutex> lock(mu);
+    if (done[device][slot] >= bytes) return GG_OK;
+    GG_CUDA(cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes), "shared memory opt-in");
+    done[device][slot] = bytes;
+    return GG_OK;
+}
+
+static uint64_t align256(uint64_t x) { return (x + 255u) & ~255ull; }
+
+// gg_splat_bin with an explicit shape (caller holds the context lock and has
+// checked the arguments).
+static int splat_bin_shaped(gg_particles* ps, gg_volume* vol, const SplatUniforms* u, uint32_t edge, uint32_t chunk) {
+    gg_context* ctx = vol->ctx;
+    if (edge == 0u) {
+        SplatArgs a{ps->pos, ps->vel, vol->sums, *u, ps->first_index};
+        bin_kernel<<<(ps->count + 255u) / 256u, 256, 0, ctx->stream>>>(a);
+        return gg::launch_status("splat bin");
+    }
+    GG_CHECK(check_shape(vol, edge, chunk));
+    const uint32_t per = bricks_per_axis(vol->size, edge);
+    const uint32_t bricks = per * per * per;
+    const uint64_t words = align256(4ull * bricks) * 2u + align256(4ull * (bricks + 1u)) * 2u;
+    const uint64_t bytes = words + align256(4ull * ps->count);
+    GG_CHECK(gg::ensure_capacity(ctx, &vol->brick_scratch, &vol->brick_scratch_capacity, bytes, "splat bricks"));
+    char* base = static_cast<char*>(vol->brick_scratch);
+    BrickArgs a;
+    a.pos = ps->pos;
+    a.vel = ps->vel;
+    a.sums = vol->sums;
+    a.u = *u;
+    a.first_index = ps->first_index;
+    a.edge = edge;
+    a.per_axis = per;
+    a.bricks = bricks;
+    a.chunk = chunk;
+    a.counts = reinterpret_cast<uint32_t*>(base);
+    a.cursor = reinterpret_cast<uint32_t*>(base + align256(4ull * bricks));
+    a.offsets = reinterpret_cast<uint32_t*>(base + 2u * align256(4ull * bricks));
+    a.items = reinterpret_cast<uint32_t*>(base + 2u * align256(4ull * bricks) + align256(4ull * (bricks + 1u)));
+    a.sorted = reinterpret_cast<uint32_t*>(base + words);
+    GG_CUDA(cudaMemsetAsync(a.counts, 0, 4ull * bricks, ctx->stream), "brick counts");
+    const int hist = (int)(4u * bricks);
+    GG_CHECK(allow_shared((const void*)brick_count_kernel, hist, ctx->device, 0));
+    GG_CHECK(allow_shared((const void*)brick_scatter_kernel, hist, ctx->device, 1));
+    const uint32_t blocks = (ps->count + kBrickParticlesPerBlock - 1u) / kBrickParticlesPerBlock;
+    brick_count_kernel<<<blocks, kBrickBlock, hist, ctx->stream>>>(a);
+    GG_CHECK(gg::launch_status("brick count"));
+    brick_scan_kernel<<<1, 1024, 0, ctx->stream>>>(a);
+    GG_CHECK(gg::launch_status("brick scan"));
+    brick_scatter_kernel<<<blocks, kBrickBlock, hist, ctx->stream>>>(a);
+    GG_CHECK(gg::launch_status("brick scatter"));
+    // Work items number at most count / chunk + one per non-empty brick.
+    const uint32_t grid = (ps->count + chunk - 1u) / chunk + bricks;
+    if (edge == 4u) {
+        brick_deposit_kernel<4><<<grid, kBrickBlock, tile_bytes<4>(), ctx->stream>>>(a);
+    } else if (edge == 8u) {
+        brick_deposit_kernel<8><<<grid, kBrickBlock, tile_bytes<8>(), ctx->stream>>>(a);
+    } else {
+        GG_CHECK(allow_shared((const void*)brick_deposit_kernel<16>, (int)tile_bytes<16>(), ctx->device, 2));
+        brick_deposit_kernel<16><<<grid, kBrickBlock, tile_bytes<16>(), ctx->stream>>>(a);
+    }
+    return gg::launch_status("brick deposit");
+}
 
 static int check_splat(const gg_particles* ps, const gg_volume* vol, const SplatUniforms* u, const char* what) {
     if (!vol || !u) return gg::fail(GG_ERR_INVALID_ARGUMENT, "%s needs a volume and uniforms.", what);
@@ -260,6 +548,7 @@ GG_API void gg_volume_destroy(gg_volume* vol) {
     if (vol->velocity) cudaFreeArray(vol->velocity);
     const uint64_t voxels = (uint64_t)vol->size * vol->size * vol->size;
     gg::device_free(ctx, vol->sums, voxels * 24u);
+    gg::device_free(ctx, vol->brick_scratch, vol->brick_scratch_capacity);
     uint64_t tex = voxels * 16u;
     ctx->used -= tex < ctx->used ? tex : ctx->used;
     delete vol;
@@ -271,9 +560,66 @@ GG_API int gg_splat_bin(gg_particles* ps, gg_volume* vol, const SplatUniforms* u
     gg_context* ctx = vol->ctx;
     std::lock_guard<std::recursive_mutex> lock(ctx->mu);
     GG_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
-    SplatArgs a{ps->pos, ps->vel, vol->sums, *u, ps->first_index};
-    bin_kernel<<<(ps->count + 255u) / 256u, 256, 0, ctx->stream>>>(a);
-    return gg::launch_status("splat bin");
+    const int mode = u->exactDeposit ? 1 : 0;
+    return splat_bin_shaped(ps, vol, u, vol->brick_edge[mode], vol->brick_chunk[mode]);
+}
+
+GG_API int gg_volume_splat_shape(gg_volume* vol, int exact, uint32_t brick_edge, uint32_t chunk) {
+    if (!vol) return gg::fail(GG_ERR_INVALID_ARGUMENT, "gg_volume_splat_shape needs a volume.");
+    GG_CHECK(check_shape(vol, brick_edge, chunk));
+    std::lock_guard<std::recursive_mutex> lock(vol->ctx->mu);
+    vol->brick_edge[exact ? 1 : 0] = brick_edge;
+    vol->brick_chunk[exact ? 1 : 0] = brick_edge ? chunk : 0u;
+    return GG_OK;
+}
+
+GG_API int gg_splat_autotune(gg_particles* ps, gg_volume* vol, const SplatUniforms* u, uint32_t* brick_edge,
+                             uint32_t* chunk, float* best_ms) {
+    if (!ps) return gg::fail(GG_ERR_INVALID_ARGUMENT, "gg_splat_autotune needs a particle system.");
+    GG_CHECK(check_splat(ps, vol, u, "gg_splat_autotune"));
+    gg_context* ctx = vol->ctx;
+    std::lock_guard<std::recursive_mutex> lock(ctx->mu);
+    GG_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
+    static const uint32_t kShapes[][2] = {{0, 0},     {4, 1024},  {4, 4096},  {8, 1024},   {8, 2048},
+                                          {8, 4096},  {8, 8192},  {16, 2048}, {16, 4096},  {16, 8192},
+                                          {16, 16384}};
+    cudaEvent_t e0, e1;
+    GG_CUDA(cudaEventCreate(&e0), "autotune events");
+    GG_CUDA(cudaEventCreate(&e1), "autotune events");
+    float best = 1e30f;
+    uint32_t best_edge = 0, best_chunk = 0;
+    int status = GG_OK;
+    for (const auto& shape : kShapes) {
+        if (check_shape(vol, shape[0], shape[1]) != GG_OK) continue;
+        float total = 0.0f;
+        for (int rep = 0; rep < 4 && status == GG_OK; ++rep) {
+            status = gg_volume_clear(vol);
+            if (status == GG_OK) status = gg::cuda_status(cudaEventRecord(e0, ctx->stream), "autotune");
+            if (status == GG_OK) status = splat_bin_shaped(ps, vol, u, shape[0], shape[1]);
+            if (status == GG_OK) status = gg::cuda_status(cudaEventRecord(e1, ctx->stream), "autotune");
+            if (status == GG_OK) status = gg::cuda_status(cudaEventSynchronize(e1), "autotune");
+            float ms = 0.0f;
+            if (status == GG_OK) status = gg::cuda_status(cudaEventElapsedTime(&ms, e0, e1), "autotune");
+            if (rep > 0) total += ms;  // the first run also grows the scratch
+        }
+        if (status != GG_OK) break;
+        if (total / 3.0f < best) {
+            best = total / 3.0f;
+            best_edge = shape[0];
+            best_chunk = shape[1];
+        }
+    }
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    GG_CHECK(status);
+    GG_CHECK(gg_volume_clear(vol));
+    const int mode = u->exactDeposit ? 1 : 0;
+    vol->brick_edge[mode] = best_edge;
+    vol->brick_chunk[mode] = best_chunk;
+    if (brick_edge) *brick_edge = best_edge;
+    if (chunk) *chunk = best_chunk;
+    if (best_ms) *best_ms = best;
+    return GG_OK;
 }
 
 GG_API int gg_splat_resolve(gg_volume* vol, const SplatUniforms* u, const gg_particles* ps) {

@@ -236,6 +236,30 @@ class Context:
         check(lib().gg_tables_read(self.handle, ptr(s), ptr(c), ptr(k)))
         return s, c, k
 
+    def atomic_peak_gadds(self, records: int = 128 ** 3) -> float:
+        """Scattered 32-bit global atomic adds per second (G/s) into a grid
+        of six-word records, the splat's ceiling."""
+        r = C.c_double()
+        check(lib().gg_measure_atomic_peak(self.handle, records, C.byref(r)))
+        return r.value
+
+    def shared_atomic_peak_gadds(self) -> float:
+        """Scattered 32-bit shared-memory atomic adds per second (G/s) into a
+        9^3 tile of six-word records, the brick splat's ceiling."""
+        r = C.c_double()
+        check(lib().gg_measure_shared_atomic_peak(self.handle, C.byref(r)))
+        return r.value
+
+    def capture_boundary(self, u: T.MarchUniforms, origin, base, axis, lo: float, hi: float, rays: int = 1024,
+                         rounds: int = 3) -> float:
+        """gg_capture_boundary: t of the capture boundary of the rays
+        origin -> base + t axis, bisected in FP64 on the device."""
+        o, b, a = (np.ascontiguousarray(v, np.float64) for v in (origin, base, axis))
+        t = C.c_double()
+        check(lib().gg_capture_boundary(self.handle, C.byref(u), ptr(o), ptr(b), ptr(a), lo, hi, rays, rounds,
+                                        C.byref(t)))
+        return t.value
+
     def fp32_peak_tflops(self) -> float:
         t = C.c_double()
         check(lib().gg_measure_fp32_peak(self.handle, C.byref(t)))
@@ -325,6 +349,17 @@ class Particles:
         check(lib().gg_particles_checksum(self.handle, C.byref(h)))
         return h.value
 
+    def seed_profile(self, fraction: float = 0.7, exponent: float = 3.0):
+        """gg_particles_seed_profile: seed `fraction` of the particles from a
+        power-law surface density ~ r^-exponent (the max preset's contention
+        workload); call before seed_particles."""
+        check(lib().gg_particles_seed_profile(self.handle, fraction, exponent))
+
+    def profile_table(self) -> np.ndarray:
+        out = np.zeros(1024, np.float32)
+        check(lib().gg_particles_profile_table(self.handle, out.ctypes.data_as(L.f32p), 1024))
+        return out
+
     def inverse_cdf(self) -> np.ndarray:
         out = np.zeros(1024, np.float32)
         check(lib().gg_particles_inverse_cdf(self.handle, out.ctypes.data_as(L.f32p), 1024))
@@ -376,6 +411,17 @@ class Volume:
     def bin(self, ps: Particles, exact: bool = True, frame: int | None = None):
         u = splat_uniforms(self.size, ps.count, ps.seed, self.frame if frame is None else frame, exact)
         check(lib().gg_splat_bin(ps.handle, self.handle, C.byref(u)))
+
+    def set_shape(self, exact: bool, brick_edge: int, chunk: int = 0):
+        """gg_volume_splat_shape: 0 = direct global atomics, else 4/8/16."""
+        check(lib().gg_volume_splat_shape(self.handle, 1 if exact else 0, brick_edge, chunk))
+
+    def autotune(self, ps: "Particles", exact: bool = True) -> tuple[int, int, float]:
+        """gg_splat_autotune: (brick edge, chunk, ms) of the fastest shape."""
+        u = splat_uniforms(self.size, ps.count, ps.seed, self.frame, exact)
+        e, c, ms = C.c_uint32(), C.c_uint32(), C.c_float()
+        check(lib().gg_splat_autotune(ps.handle, self.handle, C.byref(u), C.byref(e), C.byref(c), C.byref(ms)))
+        return e.value, c.value, ms.value
 
     def resolve(self):
         u = splat_uniforms(self.size, 0, 0)
@@ -439,6 +485,15 @@ class Targets:
         depth = np.zeros(n, np.float32)
         check(lib().gg_targets_read(self.handle, ptr(color), ptr(debug), ptr(depth), None))
         return color, debug, depth
+
+    def write(self, color: np.ndarray | None = None, debug: np.ndarray | None = None):
+        """Load width*height half4 pixels (e.g. a served request's output)."""
+        c = None if color is None else np.ascontiguousarray(color, np.float16)
+        d = None if debug is None else np.ascontiguousarray(debug, np.float16)
+        for a in (c, d):
+            if a is not None and a.size != self.width * self.height * 4:
+                raise ValueError(f"{a.size} values for a {self.width}x{self.height} half4 target")
+        check(lib().gg_targets_write(self.handle, None if c is None else ptr(c), None if d is None else ptr(d)))
 
     def tonemap(self, exposure: float = 1.0, debug_view: bool = False, drift_budget: float = DRIFT_BUDGET_INTERACTIVE):
         u = T.PresentUniforms()

@@ -156,7 +156,7 @@ class ServerConfig(C.Structure):
                 ("max_waves_in_flight", u32)]
 
 
-SERVE_BATCHED, SERVE_SERIAL_PLAIN = 0, 1
+SERVE_BATCHED, SERVE_SERIAL_PLAIN, SERVE_SERIAL_PLAIN_AS_WRITTEN = 0, 1, 2
 REQUEST_NO_STARS, REQUEST_NO_REDSHIFT = 1, 2
 
 
@@ -176,4 +176,4 @@ LAYOUT = {
 
 RAY_CAPTURED, RAY_ESCAPED, RAY_EXHAUSTED = 0, 1, 2
 POTENTIAL_NEWTONIAN, POTENTIAL_PACZYNSKI_WIITA = 0, 1
-PRECISION_PLAIN, PRECISION_COMPENSATED = 0, 1
+PRECISION_PLAIN, PRECISION_COMPENSATED, PRECISION_PLAIN_AS_WRITTEN = 0, 1, 2

@@ -105,6 +105,19 @@ GG_API void gg_particles_destroy(gg_particles* ps);
 GG_API int gg_particles_create_shard(gg_context* ctx, uint32_t count, uint32_t first_index, uint64_t seed,
                                      uint32_t potential, gg_particles** out);
 
+/* Seed a share of the particles from a second radial profile, a surface
+ * density Sigma ~ r^-exponent on [R_ISCO, R_DISK_OUTER] (rising toward the
+ * ISCO for exponent > 0): at event 0, a particle whose spare hash word (the
+ * third word of the second pcg4d draw) is below `fraction` reads its radius
+ * from this profile's inverse-CDF table instead of the steady disk's. The
+ * max preset's contention workload (70 % from a power law near r = 6) has no
+ * reference counterpart; fraction 0 restores the reference's seeding. Call
+ * before gg_particles_seed. */
+GG_API int gg_particles_seed_profile(gg_particles* ps, float fraction, float exponent);
+
+/* Copy the profile's INVERSE_CDF_COUNT-entry table (FP64 rounded to float). */
+GG_API int gg_particles_profile_table(gg_particles* ps, float* out, uint32_t count);
+
 /* The uniforms the particle kernels run with (ParticleSystem.swift:59-70). */
 GG_API int gg_particles_uniforms(gg_particles* ps, SimUniforms* out);
 
@@ -166,6 +179,23 @@ GG_API int gg_volume_read_sums(gg_volume* vol, uint32_t* emission, int32_t* mome
  * the grids of several GPUs' particle shards. */
 GG_API int gg_volume_write_sums(gg_volume* vol, const uint32_t* emission, const int32_t* momentum, const uint32_t* mass);
 
+/* How gg_splat_bin deposits, per mode (exact != 0: the exact eight-corner
+ * deposit, else the stochastic one). brick_edge 0: one thread per particle
+ * adding into the sums with global atomics. brick_edge 4, 8 or 16: the grid
+ * is cut into bricks of that edge, particles are sorted by brick, and each
+ * work item of `chunk` particles of one brick deposits into a shared-memory
+ * copy of its (edge+1)^3 voxels before adding the non-zero words to the
+ * sums. Every shape gives the same sums bit for bit. Default: edge 8, chunk
+ * 2048 (exact) and 4096 (stochastic). */
+GG_API int gg_volume_splat_shape(gg_volume* vol, int exact, uint32_t brick_edge, uint32_t chunk);
+
+/* Time gg_splat_bin under each shape on these particles (u->exactDeposit
+ * selects the mode) and keep the fastest for that mode. Outputs (each may be
+ * NULL): the chosen edge and chunk and its time in ms. The sums are left
+ * zeroed. */
+GG_API int gg_splat_autotune(gg_particles* ps, gg_volume* vol, const SplatUniforms* u, uint32_t* brick_edge,
+                             uint32_t* chunk, float* best_ms);
+
 /* Device address and length (in 32-bit words) of the volume's sums: one
  * record of six words per voxel (energy, energy*T, momentum x/y/z, mass),
  * voxel index (z n + y) n + x. Every word is a two's-complement sum, so the
@@ -208,14 +238,25 @@ GG_API void gg_targets_destroy(gg_targets* t);
 GG_API int gg_targets_read(gg_targets* t, uint16_t* color_half4, uint16_t* debug_half4, float* depth,
                            uint16_t* motion_half2);
 
-/* Precision policy of the march. */
+/* Load colour and/or debug pixels (width x height half4, NULL to skip) into
+ * the targets, e.g. a served request's output before gg_tonemap. */
+GG_API int gg_targets_write(gg_targets* t, const uint16_t* color_half4, const uint16_t* debug_half4);
+
+/* Precision policy of the march. Every policy takes the reference's steps
+ * (march.metal:51-184: the same RK4, step policy and termination), so ray
+ * step counts agree; they differ in how each step's arithmetic runs. */
 typedef enum {
-    /* FP32 RK4 exactly as the reference kernel (march.metal:51-184). */
+    /* FP32, direct state update, with this library's step arithmetic (one
+     * reciprocal per derivative, the RK4 stages as a loop, series sin/cos). */
     GG_PRECISION_PLAIN = 0,
-    /* FP32 RK4 with compensated (TwoSum) accumulation of the state update
-     * and, for Schwarzschild, rays whose drift exceeds the budget inside
+    /* The same FP32 step arithmetic with compensated (TwoSum) accumulation
+     * of the state update, and rays whose drift exceeds the budget inside
      * r < 4 re-integrated in FP64. */
-    GG_PRECISION_COMPENSATED = 1
+    GG_PRECISION_COMPENSATED = 1,
+    /* FP32 with the reference kernel's arithmetic as written: four
+     * derivative calls per step with their divides, library sin/cos
+     * (Geodesic.h:42-59, Kerr.h:63-99). The per-request baseline. */
+    GG_PRECISION_PLAIN_AS_WRITTEN = 2
 } gg_precision;
 
 /* March one image (or a tile of it: u->tileOrigin selects the tile, the
@@ -238,6 +279,22 @@ GG_API int gg_march_stats(gg_context* ctx, uint64_t* ray_steps, uint64_t* sample
  * march.metal:290-341) and Probes.run (Probes.swift:26-43). */
 GG_API int gg_probe(gg_context* ctx, const MarchUniforms* u, const RayProbe* probes, RayProbeResult* results,
                     uint32_t count, int precision);
+
+/* The capture boundary (the shadow's edge) along a one-parameter family of
+ * rays, bisected in FP64 on the device: rays leave `origin` along base + t
+ * axis for t in [lo, hi]; each round marches rays_per_round FP64 rays at the
+ * centres of equal cells of the bracket and keeps the cell pair after the
+ * last ray whose outcome (captured or not) matches the first ray's, so each
+ * round narrows the bracket by rays_per_round / 2 or more; isolated rays of
+ * the other outcome before it (a captured ray that one step carries across
+ * the horizon can end as an escape, as in the reference's integrator) do
+ * not count. A ray just past that last ray which reaches the step cap orbits
+ * on the boundary and ends the search there (the rule of
+ * Validate.swift:125-150). u supplies spin, step policy and escape radius.
+ * *t_out: the boundary's t. */
+GG_API int gg_capture_boundary(gg_context* ctx, const MarchUniforms* u, const double origin[3], const double base[3],
+                               const double axis[3], double lo, double hi, uint32_t rays_per_round, uint32_t rounds,
+                               double* t_out);
 
 /* Largest target, in pixels, gg_march_compensated_noalloc serves. */
 #define NOALLOC_MAX_PIXELS 2097152u
@@ -340,8 +397,13 @@ typedef enum {
      * re-integration of flagged rays. */
     GG_SERVE_BATCHED = 0,
     /* One request at a time through the plain FP32 image kernel
-     * (gg_march with GG_PRECISION_PLAIN), the per-request baseline. */
-    GG_SERVE_SERIAL_PLAIN = 1
+     * (gg_march with GG_PRECISION_PLAIN): what batching adds over
+     * per-request launches of the same step arithmetic. */
+    GG_SERVE_SERIAL_PLAIN = 1,
+    /* One request at a time through the image kernel with the reference's
+     * arithmetic (GG_PRECISION_PLAIN_AS_WRITTEN): the reference's
+     * per-request march. */
+    GG_SERVE_SERIAL_PLAIN_AS_WRITTEN = 2
 } gg_serve_mode;
 
 typedef struct {
@@ -383,6 +445,15 @@ GG_API int gg_server_totals(gg_server* s, int reset, uint64_t* requests, uint64_
  * every SM (each FMA counted as two flops): the peak the march's roofline is
  * quoted against. */
 GG_API int gg_measure_fp32_peak(gg_context* ctx, double* tflops);
+
+/* The device's rate, in G adds/s, of relaxed 32-bit global atomic adds into
+ * a grid of `records` six-word records (the splat's sums layout) at
+ * uniformly scattered records: the denominator of the splat's roofline. */
+GG_API int gg_measure_atomic_peak(gg_context* ctx, uint32_t records, double* gatomics);
+
+/* The same rate, in G adds/s, for 32-bit atomic adds into a shared-memory
+ * tile of 9^3 six-word records (the brick splat's tile at edge 8). */
+GG_API int gg_measure_shared_atomic_peak(gg_context* ctx, double* gatomics);
 
 #ifdef __cplusplus
 }

@@ -159,6 +159,12 @@ double o_side_ratio(const double* luminance, int width, int height);
  * particle of global index first_index + i (0 for an unsharded system). */
 void o32_seed(float* particles, uint32_t n, uint32_t seed_lo, uint32_t seed_hi, uint32_t potential,
               const float* inverse_cdf, uint32_t cdf_count, float temperature_scale, uint32_t first_index);
+/* o32_seed with a second seeding table: a seed whose third word of the
+ * second hash draw is below profile_fraction reads its radius from
+ * `profile` (the device's gg_particles_seed_profile). */
+void o32_seed_profile(float* particles, uint32_t n, uint32_t seed_lo, uint32_t seed_hi, uint32_t potential,
+                      const float* inverse_cdf, uint32_t cdf_count, float temperature_scale, uint32_t first_index,
+                      const float* profile, float profile_fraction);
 void o32_step(float* particles, uint32_t n, uint32_t seed_lo, uint32_t seed_hi, uint32_t potential,
               const float* inverse_cdf, uint32_t cdf_count, float dt, float alpha, float temperature_scale,
               uint32_t dispatches, int threads, uint32_t first_index);

@@ -57,6 +57,8 @@ typedef struct {
     uint32_t seed_lo, seed_hi, potential, cdf_count;
     const float* cdf;
     float dt, alpha, temperature_scale;
+    const float* profile; /* second seeding table or NULL */
+    float profile_fraction;
 } sim32;
 
 /* sim.metal:6-34 */
@@ -68,10 +70,11 @@ static void spawn32(uint32_t index, uint32_t event, const sim32* u, int from_dis
     float u4 = unitf(h1[0]), u5 = unitf(h1[1]);
     float r;
     if (from_disk) {
+        const float* table = (u->profile && unitf(h1[2]) < u->profile_fraction) ? u->profile : u->cdf;
         float position = u0 * (float)(u->cdf_count - 1u);
         uint32_t k = (uint32_t)position;
         if (k > u->cdf_count - 2u) k = u->cdf_count - 2u;
-        float a = u->cdf[k], b = u->cdf[k + 1u];
+        float a = table[k], b = table[k + 1u];
         r = a + (b - a) * (position - (float)k);
     } else {
         float inner = R_FEED_INNER * R_FEED_INNER;
@@ -143,14 +146,21 @@ static void step32(uint32_t i, const sim32* u, float* p) {
 
 void o32_seed(float* particles, uint32_t n, uint32_t seed_lo, uint32_t seed_hi, uint32_t potential,
               const float* cdf, uint32_t cdf_count, float temperature_scale, uint32_t first_index) {
-    sim32 u = {seed_lo, seed_hi, potential, cdf_count, cdf, 0.0f, 0.0f, temperature_scale};
+    o32_seed_profile(particles, n, seed_lo, seed_hi, potential, cdf, cdf_count, temperature_scale, first_index, NULL,
+                     0.0f);
+}
+
+void o32_seed_profile(float* particles, uint32_t n, uint32_t seed_lo, uint32_t seed_hi, uint32_t potential,
+                      const float* cdf, uint32_t cdf_count, float temperature_scale, uint32_t first_index,
+                      const float* profile, float profile_fraction) {
+    sim32 u = {seed_lo, seed_hi, potential, cdf_count, cdf, 0.0f, 0.0f, temperature_scale, profile, profile_fraction};
     for (uint32_t i = 0; i < n; ++i) spawn32(first_index + i, 0u, &u, 1, particles + 8 * (uint64_t)i);
 }
 
 void o32_step(float* particles, uint32_t n, uint32_t seed_lo, uint32_t seed_hi, uint32_t potential,
               const float* cdf, uint32_t cdf_count, float dt, float alpha, float temperature_scale,
               uint32_t dispatches, int threads, uint32_t first_index) {
-    sim32 u = {seed_lo, seed_hi, potential, cdf_count, cdf, dt, alpha, temperature_scale};
+    sim32 u = {seed_lo, seed_hi, potential, cdf_count, cdf, dt, alpha, temperature_scale, NULL, 0.0f};
 #ifdef _OPENMP
     if (threads > 0) omp_set_num_threads(threads);
 #endif

@@ -152,6 +152,7 @@ def lib() -> C.CDLL:
         "o_side_ratio": (d, [_dp, i, i]),
         "o32_seed": (None, [_fp, u32, u32, u32, u32, _fp, u32, C.c_float, u32]),
         "o32_step": (None, [_fp, u32, u32, u32, u32, _fp, u32, C.c_float, C.c_float, C.c_float, u32, i, u32]),
+        "o32_seed_profile": (None, [_fp, u32, u32, u32, u32, _fp, u32, C.c_float, u32, _fp, C.c_float]),
         "o_fnv1a": (u64, [C.c_void_p, u64]),
         "o32_deposit": (None, [_fp, u32, u32, C.c_float, C.c_float, C.c_float, u32, u32, u32, u32, _u32p, _i32p, _u32p,
                                 u32]),
@@ -266,6 +267,16 @@ def seed32(n: int, seed: int, potential: int, cdf: np.ndarray, temperature_scale
     parts = np.zeros((n, 8), np.float32)
     cdf = np.ascontiguousarray(cdf, np.float32)
     lib().o32_seed(parts, n, seed & 0xFFFFFFFF, seed >> 32, potential, cdf, len(cdf), temperature_scale, first_index)
+    return parts
+
+
+def seed32_profile(n: int, seed: int, potential: int, cdf: np.ndarray, temperature_scale: float,
+                   profile: np.ndarray, fraction: float, first_index: int = 0) -> np.ndarray:
+    parts = np.zeros((n, 8), np.float32)
+    cdf = np.ascontiguousarray(cdf, np.float32)
+    profile = np.ascontiguousarray(profile, np.float32)
+    lib().o32_seed_profile(parts, n, seed & 0xFFFFFFFF, seed >> 32, potential, cdf, len(cdf), temperature_scale,
+                           first_index, profile, fraction)
     return parts
 
 

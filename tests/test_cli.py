@@ -1,0 +1,67 @@
+"""The command line's parser and exit codes (Options.swift:60-154,
+Exit.swift:5-18), on the CPU: nothing here touches a GPU."""
+import subprocess
+import sys
+
+import pytest
+
+from gargantua_b200 import cli
+
+
+def test_defaults_follow_the_reference():
+    o = cli.parse([])
+    assert o.command == "interactive" and o.preset == "default" and o.seed == 1
+    assert (o.width, o.height) == (3840, 2160) and o.spin == 0.0 and o.strategy == "march"
+    assert o.configuration == (1_000_000, 128, 960, 540)
+
+
+def test_still_with_overrides():
+    o = cli.parse(["--still", "x.png", "--width", "640", "--height", "360", "--spin", "0.9", "--camera",
+                   "1.0,0.4,40", "--seed", "18446744073709551615", "--preset", "small", "--volume", "192",
+                   "--sequence", "3"])
+    assert o.command == "still" and o.still_path == "x.png"
+    assert (o.width, o.height, o.spin, o.camera, o.sequence) == (640, 360, 0.9, (1.0, 0.4, 40.0), 3)
+    assert o.seed == 2**64 - 1
+    assert o.configuration == (250_000, 192, 640, 360)
+
+
+@pytest.mark.parametrize("argv,fragment", [
+    (["--preset", "huge"], "unknown preset"),
+    (["--volume", "100"], "volume must be"),
+    (["--seed", "-1"], "seed must be"),
+    (["--seed", str(2**64)], "seed must be"),
+    (["--strategy", "trace"], "unknown strategy"),
+    (["--fps-cap", "45"], "fps cap"),
+    (["--width", "0"], "positive integer"),
+    (["--spin", "0.999"], "spin must be"),
+    (["--camera", "1,2,60"], "camera needs"),
+    (["--camera", "1,2"], "camera needs"),
+    (["--still"], "needs a value"),
+    (["--frobnicate"], "unknown argument"),
+])
+def test_refusals(argv, fragment):
+    with pytest.raises(cli.UsageError, match=fragment):
+        cli.parse(argv)
+
+
+def test_camera_clamps_elevation():
+    cam = cli.orbit_camera(cli.parse(["--camera", "0.5,3.0,30"]))
+    assert cam.elevation == 1.5 and cam.distance == 30.0 and cam.azimuth == 0.5
+
+
+def _run(*args):
+    return subprocess.run([sys.executable, "-m", "gargantua_b200", *args], capture_output=True, text=True,
+                          cwd=cli.os.path.dirname(cli.os.path.dirname(cli.__file__)))
+
+
+def test_exit_codes_and_simple_commands():
+    r = _run("--volume", "7")
+    assert r.returncode == 64 and "volume must be" in r.stderr
+    r = _run("version")
+    assert r.returncode == 0 and r.stdout.startswith("gargantua-b200 ")
+    r = _run("constants")
+    assert r.returncode == 0 and "#define STEP_CAP_STILL" in r.stdout
+    r = _run()
+    assert r.returncode == 2 and "display" in r.stderr
+    r = _run("validate")
+    assert r.returncode == 2 and "pytest" in r.stderr

@@ -350,3 +350,75 @@ def test_kerr_probe_parity_against_fp64_oracle(world):
         d = np.linalg.norm(ref[esc, :3] - gpu["position"][esc].astype(np.float64), axis=1) / np.maximum(
             np.linalg.norm(ref[esc, :3], axis=1), 1.0)
         assert d.max() < 1e-3, (prec, float(d.max()))
+
+
+# The per-request baseline with the reference's step arithmetic as written
+# (GG_PRECISION_PLAIN_AS_WRITTEN) meets the same bars.
+
+AS_WRITTEN = 2
+
+
+@pytest.mark.parametrize("name,settings", [("conservation_interactive", "interactive"),
+                                           ("conservation_still", "still")])
+def test_conservation_as_written(world, name, settings):
+    import gargantua_b200 as g
+
+    golden = load_golden(name)
+    st = getattr(g.Settings, settings)()
+    launches = g.camera_grid(g.OrbitCamera(), int(golden["parameters"]["columns"]), int(golden["parameters"]["rows"]),
+                             960 / 540)
+    res = world["ctx"].probe(launches, probe_uniforms(g, world["ctx"], st), AS_WRITTEN)
+    worst = float(res["drift"].max())
+    assert golden_passes(golden, worst), f"max drift {worst:.2e}"
+
+
+def test_parity_as_written(world):
+    import gargantua_b200 as g
+
+    golden = load_golden("parity")
+    launches = [g.as_float32_launch(l) for l in g.camera_grid(g.OrbitCamera(), 8, 8, 960 / 540)]
+    gpu = world["ctx"].probe(launches, probe_uniforms(g, world["ctx"], g.Settings.still()), AS_WRITTEN)
+    probes = np.array([np.concatenate([l.origin, l.direction]) for l in launches])
+    ref = O.integrate_batch(probes, O.still(), THREADS)
+    dist = np.linalg.norm(ref[:, :3] - gpu["position"].astype(np.float64), axis=1) / np.maximum(
+        np.linalg.norm(ref[:, :3], axis=1), 1.0)
+    mismatches = int((ref[:, 7].astype(int) != gpu["outcome"].astype(int)).sum())
+    assert golden_passes(golden, float(dist.max())) and mismatches == 0, (float(dist.max()), mismatches)
+
+
+# The capture boundary bisected in FP64 on the device (gg_capture_boundary).
+
+def test_capture_boundary_fp64_schwarzschild(world):
+    """The shadow golden's edge, b_c = 3 sqrt 3, from FP64 rays on the GPU."""
+    import gargantua_b200 as g
+
+    golden = load_golden("shadow")
+    radius = float(golden["parameters"]["launchRadius"])
+    u = probe_uniforms(g, world["ctx"], g.Settings.still())
+    t = world["ctx"].capture_boundary(u, [radius, 0.0, 0.0], [-1.0, 0.0, 0.0], [0.0, 1.0, 0.0], 0.0, 0.5, 1024, 3)
+    ray = O.launch([radius, 0.0, 0.0], [-1.0, t, 0.0])
+    b = ray.angular_momentum / ray.energy
+    assert golden_passes(golden, b), f"b = {b:.6f}"
+    assert abs(b - 3.0 * math.sqrt(3.0)) < 2e-3, b
+
+
+def test_capture_boundary_fp64_kerr_matches_the_oracle(world):
+    """Prograde and retrograde equatorial edges at spin 0.9 against the
+    oracle's FP64 bisection (KerrGeodesic.swift), same launch family."""
+    import ctypes as C
+
+    import gargantua_b200 as g
+
+    golden = load_golden("shadow_kerr")
+    p = golden["parameters"]
+    spin, radius = p["spin"], p["launchRadius"]
+    u = probe_uniforms(g, world["ctx"], g.Settings.still(), spin=spin)
+    st = O.kerr_settings(4096)
+    for side in (1.0, -1.0):
+        t = world["ctx"].capture_boundary(u, [radius, 0.0, 0.0], [-1.0, 0.0, 0.0], [0.0, side, 0.0], 0.0,
+                                          12.0 / radius, 1024, 4)
+        s = np.zeros(7)
+        O.lib().o_kerr_launch(spin, np.array([radius, 0.0, 0.0]), np.array([-1.0, side * t, 0.0]), s)
+        xi = s[6] / s[5]
+        ref = O.lib().o_kerr_bisect_critical_xi(spin, radius, side, C.byref(st), 48)
+        assert abs(xi - ref) <= 1e-4 * abs(ref), (side, xi, ref)

@@ -45,12 +45,13 @@ def run(server, specs, debug=False):
     return [server.wait(t) for t in tickets]
 
 
-def test_served_matches_plain_per_request(world):
+@pytest.mark.parametrize("mode", ["SERVE_SERIAL_PLAIN", "SERVE_SERIAL_PLAIN_AS_WRITTEN"])
+def test_served_matches_plain_per_request(world, mode):
     import gargantua_b200 as g
 
     specs = mix_specs()
     batched = g.Server(world["ctx"], world["vol"], g.types.SERVE_BATCHED)
-    plain = g.Server(world["ctx"], world["vol"], g.types.SERVE_SERIAL_PLAIN)
+    plain = g.Server(world["ctx"], world["vol"], getattr(g.types, mode))
     a = run(batched, specs, debug=True)
     b = run(plain, specs, debug=True)
     for spec, (pa, da, ra), (pb, db, rb) in zip(specs, a, b):
@@ -136,4 +137,20 @@ def test_invalid_requests_are_refused(world):
         assert e.value.status == 1
     totals = server.totals()
     assert totals["requests"] == 0
+    server.close()
+
+
+def test_server_autotune_picks_a_measured_candidate(world):
+    import gargantua_b200 as g
+    from gargantua_b200 import autotune
+
+    specs = mix_specs()[:4]
+    tuned = autotune.tune_server(world["ctx"], world["vol"], specs, chunks=(32, 64), waves=(1 << 20,),
+                                 in_flight=(2,), repeats=1)
+    assert tuned["chunk_rays"] in (32, 64) and tuned["rate"] > 0.0
+    assert len(tuned["trials"]) == 2 and max(t["rate"] for t in tuned["trials"]) == tuned["rate"]
+    server = g.Server(world["ctx"], world["vol"], g.types.SERVE_BATCHED, chunk_rays=tuned["chunk_rays"],
+                      wave_rays=tuned["wave_rays"], max_waves_in_flight=tuned["max_waves_in_flight"])
+    pixels, _, res = server.wait(server.submit(specs[0]))
+    assert res.status == 0 and res.counters.rays == specs[0].width * specs[0].height
     server.close()

@@ -117,3 +117,29 @@ def test_invalid_arguments_are_reported_not_trapped(ctx):
         g.Particles(small, 1_000_000)
     assert e.value.status == 3  # over budget, refused before allocating
     small.close()
+
+
+def test_concentrated_seed_profile_is_bit_exact_and_concentrated(ctx):
+    """The max preset's contention workload: 70 % of seeds from a power-law
+    surface density ~ r^-3, against the replica with the same table."""
+    import gargantua_b200 as g
+
+    n = 40000
+    ps = g.Particles(ctx, n, seed=5)
+    ps.seed_profile(0.7, 3.0)
+    table = ps.profile_table()
+    assert table[0] == np.float32(6.0) and table[-1] == np.float32(24.0) and np.all(np.diff(table) > 0)
+    # The table is Sigma ~ r^-3's inverse CDF: r(u) = (6^-1 + u (24^-1 - 6^-1))^-1.
+    u_k = np.arange(1024) / 1023.0
+    assert np.allclose(table, 1.0 / (1 / 6 + u_k * (1 / 24 - 1 / 6)), rtol=1e-6)
+    ps.seed_particles()
+    dev = ps.read()
+    u, cdf = replica_args(ps)
+    ref = O.seed32_profile(n, 5, 1, cdf, u.temperatureScale, table, 0.7)
+    assert np.array_equal(dev.view(np.uint32), ref.view(np.uint32))
+    plain = O.seed32(n, 5, 1, cdf, u.temperatureScale)
+    r_dev = np.hypot(dev[:, 0], dev[:, 1])
+    r_plain = np.hypot(plain[:, 0], plain[:, 1])
+    assert np.median(r_dev) < np.median(r_plain) - 1.0  # pulled toward the ISCO
+    ps.step(20)  # respawns ignore the profile; the step runs as before
+    ps.close()

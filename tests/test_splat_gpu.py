@@ -117,3 +117,50 @@ def test_size_mismatch_is_an_argument_error(ctx, settled):
     u = g.splat_uniforms(16, settled.count, 1)
     status = _lib.lib().gg_splat(settled.handle, vol.handle, C.byref(u))
     assert status == 1
+
+
+SHAPES = [(0, 0), (4, 1024), (8, 64), (8, 2048), (16, 4096), (16, 100000)]
+
+
+@pytest.mark.parametrize("shape", SHAPES, ids=[f"edge{e}-chunk{c}" for e, c in SHAPES])
+@pytest.mark.parametrize("size", [100, 128])
+@pytest.mark.parametrize("exact", [True, False])
+def test_every_splat_shape_is_bit_exact(ctx, settled, shape, size, exact):
+    """Direct atomics and the brick-privatised deposit (ragged last bricks at
+    100^3, many work items per brick at chunk 64) give the replica's grids."""
+    import gargantua_b200 as g
+
+    vol = g.Volume(ctx, size)
+    vol.set_shape(exact, *shape)
+    vol.bin(settled, exact=exact, frame=5)
+    em, mo, ma = vol.read_sums()
+    rem, rmo, rma = O.deposit32(settled.read(), size, frame=5, exact=exact, seed=1)
+    assert ma.sum() > 0
+    assert np.array_equal(em, rem) and np.array_equal(mo, rmo) and np.array_equal(ma, rma)
+    vol.close()
+
+
+def test_shapes_refused_outside_their_limits(ctx):
+    import gargantua_b200 as g
+
+    vol = g.Volume(ctx, 256)
+    for edge, chunk in [(5, 1024), (8, 0), (4, 1024)]:  # 64^3 bricks of edge 4 exceed the histogram
+        with pytest.raises(g.GargantuaError):
+            vol.set_shape(True, edge, chunk)
+    vol.set_shape(True, 16, 4096)
+    vol.close()
+
+
+def test_autotune_keeps_a_valid_shape_and_zeroed_sums(ctx, settled):
+    import gargantua_b200 as g
+
+    vol = g.Volume(ctx, 64)
+    edge, chunk, ms = vol.autotune(settled, exact=True)
+    assert edge in (0, 4, 8, 16) and ms > 0.0
+    em, mo, ma = vol.read_sums()
+    assert not em.any() and not mo.any() and not ma.any()
+    vol.bin(settled, exact=True, frame=2)
+    em, mo, ma = vol.read_sums()
+    rem, rmo, rma = O.deposit32(settled.read(), 64, frame=2, exact=True, seed=1)
+    assert np.array_equal(em, rem) and np.array_equal(mo, rmo) and np.array_equal(ma, rma)
+    vol.close()
