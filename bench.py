@@ -220,6 +220,51 @@ def cpu_sample(slices, seconds: float, threads: int):
     return total_steps / max(elapsed, 1e-9), total_rays, total_steps, elapsed, desc
 
 
+def drift_vs_oracle(ctx, slices, per_request: int = 64, max_requests: int = 24) -> dict:
+    """4096-step rays of the timed requests, 64 per request from a 64x36 grid
+    of its camera: drift of the compensated FP32 march (gg_probe, the served
+    arithmetic, FP64 re-integration off) beside the FP64 oracle's drift for
+    the same rays (Schwarzschild: E and L; Kerr: Carter constant and null
+    residual, each the maximum over the ray's steps as the reference
+    defines it)."""
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_ffi as O
+
+    import gargantua_b200 as g
+
+    rng = np.random.default_rng(11)
+    picked = [q for s in slices for q in s if q["step_cap"] == 4096][:max_requests]
+    out = {}
+    for kind in ("schwarzschild", "kerr"):
+        gpu, ref = [], []
+        for q in picked:
+            if (q["spin"] > 0.0) != (kind == "kerr"):
+                continue
+            cam = g.OrbitCamera(q["azimuth"], q["elevation"], q["distance"])
+            launches = g.camera_grid(cam, 64, 36, q["width"] / q["height"])
+            pick = rng.choice(len(launches), size=per_request, replace=False)
+            sel = [g.as_float32_launch(launches[i]) for i in pick]
+            escape = max(60.0, q["distance"] + 10.0)
+            st = g.Settings.still()
+            st.escape_radius = escape
+            u = g.uniforms(cam, 1, 1, st, 1.0, False, 0, spin=q["spin"])  # budget 1: no FP64 pass
+            gpu.append(ctx.probe(sel, u, g.types.PRECISION_COMPENSATED)["drift"].astype(np.float64))
+            probes = np.array([np.concatenate([l.origin, l.direction]) for l in sel])
+            if kind == "kerr":
+                res = O.kerr_integrate_batch(q["spin"], probes, O.KerrSettings(0.02, 0.005, 0.5, 0.05, escape, 4096))
+            else:
+                res = O.integrate_batch(probes, O.Settings(0.02, 0.02, 0.5, 2.02, escape, 4096, 0.06, 1.5))
+            ref.append(res[:, 6])
+        if not gpu:
+            continue
+        a, b = np.concatenate(gpu), np.concatenate(ref)
+        out[kind] = {"rays": int(a.size), "fp32_compensated": {"p50": float(np.median(a)), "p99": float(np.quantile(a, 0.99)),
+                                                               "under_1e-5": float(np.mean(a < 1e-5))},
+                     "fp64_oracle": {"p50": float(np.median(b)), "p99": float(np.quantile(b, 0.99)),
+                                     "under_1e-5": float(np.mean(b < 1e-5))}}
+    return out
+
+
 def measured_peaks() -> dict:
     path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "MEASURED_PEAKS.json")
     try:
@@ -406,7 +451,8 @@ def main():
     # Weak scaling: every rank serves its own stream (seed 1 + rank).
     stream = make_stream(1 + rank)
     slices = [stream[i * B:(i + 1) * B] for i in range(nslices)]
-    shape = {"chunk_rays": 32, "wave_rays": 4 << 20, "max_waves_in_flight": 2, "chosen_by": "defaults"}
+    shape = {"chunk_rays": 32, "wave_rays": 4 << 20, "max_waves_in_flight": 2, "steps_per_round": 8, "refill_idle": 8,
+             "chosen_by": "defaults"}
     if not args.no_tune:
         # Untimed: the server's wave shape from a sample of other requests
         # with the same mix (a different stream seed).
@@ -414,10 +460,11 @@ def main():
 
         sample = [spec_of(q) for q in make_stream(1000 + rank)[:16]]
         tuned = autotune.tune_server(ctx, vol, sample)
-        shape = {k: tuned[k] for k in ("chunk_rays", "wave_rays", "max_waves_in_flight")}
+        shape = {k: tuned[k] for k in ("chunk_rays", "wave_rays", "max_waves_in_flight", "steps_per_round",
+                                         "refill_idle")}
         shape["chosen_by"] = "gargantua_b200.autotune.tune_server on 16 requests of stream seed 1000"
-    batched = g.Server(ctx, vol, g.types.SERVE_BATCHED, chunk_rays=shape["chunk_rays"], wave_rays=shape["wave_rays"],
-                       max_waves_in_flight=shape["max_waves_in_flight"])
+    batched = g.Server(ctx, vol, g.types.SERVE_BATCHED,
+                       **{k: v for k, v in shape.items() if k != "chosen_by"})
 
     def barrier():
         torch.cuda.synchronize()
@@ -511,6 +558,8 @@ def main():
 
     passes = measure_passes(ctx, g, torch) if not args.no_passes else None
 
+    drift_oracle = drift_vs_oracle(ctx, timed) if (rank == 0 and world == 1) else None
+
     cpu = None
     if rank == 0 and world == 1:
         threads = os.cpu_count() or 1
@@ -540,7 +589,7 @@ def main():
         "p99_ms": p99,
         "plain_per_request": plain,
         "plain_lane_per_request": plain_lane,
-        "drift": {"rays": rays_total, "over_budget": drift_over},
+        "drift": {"rays": rays_total, "over_budget": drift_over, "vs_fp64_oracle": drift_oracle},
         "e2e": {"value": e2e, "unit": "ray-steps/s", "h2d_bytes_per_step": int(B * 64),
                 "d2h_bytes_per_step": int(d2h / max(args.steps, 1))},
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",

@@ -83,6 +83,7 @@ SIGNATURES = {
     "gg_volume_write": (i, [vp, vp, vp]),
     "gg_tables_update": (i, [vp, C.c_float, P(T.MarchUniforms)]),
     "gg_tables_read": (i, [vp, vp, vp, vp]),
+    "gg_context_set_fp64_policy": (i, [vp, i]),
     "gg_targets_create": (i, [vp, u32, u32, P(vp)]),
     "gg_targets_destroy": (None, [vp]),
     "gg_targets_read": (i, [vp, vp, vp, vp, vp]),
@@ -104,6 +105,7 @@ SIGNATURES = {
     "gg_server_create": (i, [vp, vp, P(T.ServerConfig), P(vp)]),
     "gg_server_destroy": (None, [vp]),
     "gg_server_submit": (i, [vp, P(T.Request), P(u64)]),
+    "gg_server_inject_fault": (i, [vp, i]),
     "gg_server_poll": (i, [vp, u64, P(i)]),
     "gg_server_wait": (i, [vp, u64, C.c_double, P(T.RequestResult)]),
     "gg_server_totals": (i, [vp, i, P(u64), P(u64), P(u64), P(C.c_double), P(C.c_double)]),

@@ -23,6 +23,7 @@ from . import types as T
 CHUNKS = (32, 64, 128)
 WAVES = (2 << 20, 4 << 20, 8 << 20)
 IN_FLIGHT = (2, 3)
+CADENCES = ((8, 8), (4, 4), (16, 8), (8, 16))  # (steps_per_round, refill_idle)
 
 
 @dataclass
@@ -30,12 +31,19 @@ class ServerShape:
     chunk_rays: int
     wave_rays: int
     max_waves_in_flight: int
+    steps_per_round: int
+    refill_idle: int
     span_seconds: float
     ray_steps: int
 
     @property
     def rate(self) -> float:
         return self.ray_steps / self.span_seconds if self.span_seconds > 0 else 0.0
+
+    def config(self) -> dict:
+        return {"chunk_rays": self.chunk_rays, "wave_rays": self.wave_rays,
+                "max_waves_in_flight": self.max_waves_in_flight, "steps_per_round": self.steps_per_round,
+                "refill_idle": self.refill_idle}
 
 
 def tune_splat(ps: H.Particles, vol: H.Volume) -> dict:
@@ -48,38 +56,46 @@ def tune_splat(ps: H.Particles, vol: H.Volume) -> dict:
     return out
 
 
-def _serve(ctx: H.Context, vol, specs, chunk: int, wave: int, flight: int, memory_bytes: int) -> ServerShape:
-    server = H.Server(ctx, vol, T.SERVE_BATCHED, memory_bytes=memory_bytes, wave_rays=wave, chunk_rays=chunk,
-                      max_waves_in_flight=flight)
+def _serve(ctx: H.Context, vol, specs, shape: dict, memory_bytes: int) -> ServerShape:
+    server = H.Server(ctx, vol, T.SERVE_BATCHED, memory_bytes=memory_bytes, **shape)
     try:
         server.totals(reset=True)
         tickets = [server.submit(s) for s in specs]
         steps = sum(int(server.wait(t)[2].ray_steps) for t in tickets)
         tot = server.totals(reset=True)
-        return ServerShape(chunk, wave, flight, tot["span_seconds"], steps)
+        return ServerShape(shape["chunk_rays"], shape["wave_rays"], shape["max_waves_in_flight"],
+                           shape["steps_per_round"], shape["refill_idle"], tot["span_seconds"], steps)
     finally:
         server.close()
 
 
 def tune_server(ctx: H.Context, vol, specs: list[H.RequestSpec], memory_bytes: int = 0, chunks=CHUNKS, waves=WAVES,
-                in_flight=IN_FLIGHT, repeats: int = 2) -> dict:
-    """The fastest (chunk_rays, wave_rays, max_waves_in_flight) for `specs`,
-    as ServerConfig keyword arguments, plus every candidate's rate."""
+                in_flight=IN_FLIGHT, cadences=CADENCES, repeats: int = 2) -> dict:
+    """The fastest server shape for `specs`, found one group of settings at
+    a time (chunk and waves in flight, then wave size, then the refill
+    cadence), as ServerConfig keyword arguments, plus every trial's rate."""
     if not specs:
         raise ValueError("tune_server needs a sample of requests")
-    _serve(ctx, vol, specs[:2], CHUNKS[0], WAVES[0], IN_FLIGHT[0], memory_bytes)  # build kernels, graphs, pools
+    best = {"chunk_rays": chunks[0], "wave_rays": waves[len(waves) // 2], "max_waves_in_flight": in_flight[0],
+            "steps_per_round": cadences[0][0], "refill_idle": cadences[0][1]}
+    _serve(ctx, vol, specs[:2], best, memory_bytes)  # build kernels, graphs, pools
     trials = []
-    for chunk in chunks:
-        for wave in waves:
-            for flight in in_flight:
-                best = None
-                for _ in range(repeats):
-                    r = _serve(ctx, vol, specs, chunk, wave, flight, memory_bytes)
-                    if best is None or r.span_seconds < best.span_seconds:
-                        best = r
-                trials.append(best)
-    win = max(trials, key=lambda t: t.rate)
-    return {"chunk_rays": win.chunk_rays, "wave_rays": win.wave_rays, "max_waves_in_flight": win.max_waves_in_flight,
-            "rate": win.rate,
-            "trials": [{"chunk_rays": t.chunk_rays, "wave_rays": t.wave_rays,
-                        "max_waves_in_flight": t.max_waves_in_flight, "rate": t.rate} for t in trials]}
+
+    def measure(shape):
+        r = min((_serve(ctx, vol, specs, shape, memory_bytes) for _ in range(repeats)), key=lambda t: t.span_seconds)
+        trials.append(r)
+        return r
+
+    groups = [
+        [{"chunk_rays": c, "max_waves_in_flight": f} for c in chunks for f in in_flight],
+        [{"wave_rays": w} for w in waves],
+        [{"steps_per_round": spr, "refill_idle": idle} for spr, idle in cadences],
+    ]
+    for group in groups:
+        results = []
+        for change in group:
+            shape = dict(best, **change)
+            results.append(measure(shape))
+        best = max(results, key=lambda t: t.rate).config()
+    win = max((t for t in trials if t.config() == best), key=lambda t: t.rate)
+    return dict(best, rate=win.rate, trials=[dict(t.config(), rate=t.rate) for t in trials])

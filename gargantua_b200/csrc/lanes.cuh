@@ -371,7 +371,7 @@ template <typename R> struct KState {
 };
 
 template <typename R> struct KConst {
-    R a, a2, E, L, aE, aL, L2, a2E2, two_aEL;
+    R a, a2, E, L, aE, aL, L2, a2E2, two_aEL, four_E;
 };
 
 template <typename R> __device__ __forceinline__ KConst<R> k_const(R a, R E, R L) {
@@ -385,6 +385,7 @@ template <typename R> __device__ __forceinline__ KConst<R> k_const(R a, R E, R L
     k.L2 = L * L;
     k.a2E2 = k.a2 * E * E;
     k.two_aEL = R(2) * a * E * L;
+    k.four_E = R(4) * E;
     return k;
 }
 
@@ -410,32 +411,34 @@ template <typename R> __device__ __forceinline__ R k_sin2(R st) { return gmax(st
 template <typename R>
 __device__ __forceinline__ KState<R> k_derivative(const KConst<R>& k, const KState<R>& s, R st, R ct, R* F_out,
                                                   R* inv_sin2_out) {
-    R r = s.r;
-    R r2 = r * r;
-    R delta = r2 - R(2) * r + k.a2;
-    R sigma = fmaT(k.a2, ct * ct, r2);
-    R inv_sigma = rcp(sigma);
-    R inv_delta = rcp(delta);
-    R sin2 = k_sin2(st);
+    const R r = s.r;
+    const R r2 = r * r;
+    const R delta = fmaT(r, r - R(2), k.a2);  // r^2 - 2r + a^2
+    const R sigma = fmaT(k.a2, ct * ct, r2);
+    const R inv_sigma = rcp(sigma);
+    const R inv_delta = rcp(delta);
+    const R sin2 = k_sin2(st);
     R inv_sin2, inv_sc;
     k_sin_inverses(st, &inv_sin2, &inv_sc);
-    R p = fmaT(r2 + k.a2, k.E, -k.aL);
-    R g = fmaT(k.a2E2, sin2, fmaT(k.L2, inv_sin2, -k.two_aEL));
-    R pr2 = s.pr * s.pr;
-    R p2d = p * p * inv_delta;
-    R F = fmaT(delta, pr2, fmaT(s.pt, s.pt, g - p2d));
-    R ham = R(0.5) * F * inv_sigma;
+    const R p = fmaT(r2 + k.a2, k.E, -k.aL);
+    const R g = fmaT(k.a2E2, sin2, fmaT(k.L2, inv_sin2, -k.two_aEL));
+    const R pr2 = s.pr * s.pr;
+    const R p2d = p * p * inv_delta;
+    const R F = fmaT(delta, pr2, fmaT(s.pt, s.pt, g - p2d));
     *F_out = F;
     *inv_sin2_out = inv_sin2;
-    R dprime = R(2) * r - R(2);
-    R fr = fmaT(dprime, pr2, inv_delta * (p2d * dprime - R(4) * r * k.E * p));
-    R fth = R(2) * ct * fmaT(k.a2E2, st, -k.L2 * inv_sin2 * inv_sc);
+    // With 2H = F / Sigma: dp_r = (2 r H - fr / 2) / Sigma, and
+    // dp_theta = (-2 a^2 sin cos H - fth / 2) / Sigma where
+    // fth / 2 = cos (a^2 E^2 sin - L^2 / (sin^2 |sin|)).
+    const R two_h = F * inv_sigma;
+    const R dprime = fmaT(R(2), r, R(-2));
+    const R fr = fmaT(dprime, pr2, inv_delta * fmaT(p2d, dprime, -k.four_E * r * p));
     KState<R> o;
     o.r = delta * s.pr * inv_sigma;
     o.th = s.pt * inv_sigma;
     o.ph = (fmaT(k.a, p * inv_delta, k.L * inv_sin2) - k.aE) * inv_sigma;
-    o.pr = (R(2) * r * ham - R(0.5) * fr) * inv_sigma;
-    o.pt = (R(-2) * k.a2 * st * ct * ham - R(0.5) * fth) * inv_sigma;
+    o.pr = fmaT(r, two_h, R(-0.5) * fr) * inv_sigma;
+    o.pt = -ct * fmaT(k.a2 * st, two_h, fmaT(k.a2E2, st, -k.L2 * inv_sin2 * inv_sc)) * inv_sigma;
     return o;
 }
 
@@ -499,6 +502,7 @@ __device__ __forceinline__ KState<R> k_increment(const KConst<R>& k, const KStat
         if (stage == 0 && gauged) *gauge = gmax(*gauge, k_gauge(k, s, ct, F, inv_sin2, carter0));
         R wk = (stage == 0 || stage == 3) ? R(1) : R(2);
         acc = k_offset(acc, d, wk);
+        if (stage == 3) break;
         const R wx = stage < 2 ? R(0.5) * h : h;
         x = k_offset(s, d, wx);
         shift = d.th * wx;

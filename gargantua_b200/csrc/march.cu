@@ -29,7 +29,7 @@ __global__ void __launch_bounds__(64) march_image_kernel(MarchParams p) {
         else r = shade_pixel<float, false>(p, px, py);
         const uint32_t local = gy * p.target_width + gx;
         write_pixel(p, local, r);
-        if (Comp && p.flagged && needs_fp64(p.u, r)) {
+        if (Comp && p.flagged && needs_fp64(p.u, r, p.fp64_all != 0u)) {
             uint32_t slot = atomicAdd(p.flagged_count, 1u);
             if (slot < p.flagged_capacity) p.flagged[slot] = local;
         }
@@ -157,7 +157,11 @@ __global__ void __launch_bounds__(64) probe_kernel(MarchParams p, const RayProbe
         r = probe_one<float, false>(p, q, &min_r);
     } else {
         r = probe_lane<float, Comp>(p, q, &min_r);
-        if (Comp && r.drift > p.u.driftBudget && min_r < 4.0f) r = probe_lane<double, false>(p, q, &min_r);
+        PixelResult pr{};
+        pr.drift = r.drift;
+        pr.min_r = min_r;
+        pr.outcome = r.outcome;
+        if (Comp && needs_fp64(p.u, pr, p.fp64_all != 0u)) r = probe_lane<double, false>(p, q, &min_r);
     }
     results[i] = r;
 }
@@ -207,6 +211,7 @@ MarchParams make_params(gg_context* ctx, const gg_volume* vol, const MarchUnifor
     p.emission = vol ? vol->emission_tex : 0;
     p.velocity = vol ? vol->velocity_tex : 0;
     p.blackbody = ctx->blackbody;
+    p.fp64_all = ctx->fp64_policy == GG_FP64_ALL_FLAGGED ? 1u : 0u;
     return p;
 }
 
@@ -310,6 +315,14 @@ GG_API int gg_targets_read(gg_targets* t, uint16_t* color, uint16_t* debug, floa
     if (depth) GG_CUDA(cudaMemcpyAsync(depth, t->depth, px * 4u, cudaMemcpyDeviceToHost, ctx->stream), "target readback");
     if (motion) GG_CUDA(cudaMemcpyAsync(motion, t->motion, px * 4u, cudaMemcpyDeviceToHost, ctx->stream), "target readback");
     GG_CUDA(cudaStreamSynchronize(ctx->stream), "target readback");
+    return GG_OK;
+}
+
+GG_API int gg_context_set_fp64_policy(gg_context* ctx, int policy) {
+    if (!ctx || (policy != GG_FP64_ESCAPING && policy != GG_FP64_ALL_FLAGGED))
+        return gg::fail(GG_ERR_INVALID_ARGUMENT, "gg_context_set_fp64_policy needs a context and a known policy.");
+    std::lock_guard<std::recursive_mutex> lock(ctx->mu);
+    ctx->fp64_policy = policy;
     return GG_OK;
 }
 

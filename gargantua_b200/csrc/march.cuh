@@ -29,6 +29,7 @@ struct MarchParams {
     uint32_t* flagged;        // FP64 re-integration list (target-local pixel indices)
     uint32_t* flagged_count;  // its length, a device counter
     uint32_t flagged_capacity;
+    uint32_t fp64_all;        // GG_FP64_ALL_FLAGGED: captured rays are re-integrated too
 };
 
 struct MarchResult {
@@ -375,8 +376,10 @@ __device__ __forceinline__ void write_pixel(const MarchParams& p, uint32_t local
 
 // A ray the compensated FP32 march flags for FP64 re-integration: over the
 // drift budget after passing inside r = 4.
-__device__ __forceinline__ bool needs_fp64(const MarchUniforms& u, const PixelResult& r) {
-    return r.drift > u.driftBudget && r.min_r < 4.0f;
+// FP64 re-integration: over the drift budget after passing inside r < 4,
+// and (unless every flagged ray is asked for) not captured.
+__device__ __forceinline__ bool needs_fp64(const MarchUniforms& u, const PixelResult& r, bool all) {
+    return r.drift > u.driftBudget && r.min_r < 4.0f && (all || r.outcome != RayCaptured);
 }
 
 }  // namespace gg

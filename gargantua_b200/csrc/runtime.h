@@ -73,6 +73,7 @@ struct gg_context {
     // Small per-call device scratch: counters and the probe buffers.
     MarchCounters* counters = nullptr;
     unsigned long long* stats = nullptr;  // last march: ray steps, samples, FP64 rays, spare
+    int fp64_policy = 0;  // gg_fp64_policy of gg_march and gg_probe
     void* probe_buffer = nullptr;
     uint64_t probe_capacity = 0;  // bytes
     uint32_t* flagged = nullptr;  // FP64 re-integration list

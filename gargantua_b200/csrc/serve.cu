@@ -52,7 +52,9 @@ struct ServeRequest {
     ushort4* color;
     ushort4* debug;
     unsigned long long* stats;  // steps, samples, fp64, rays, over budget, exhausted, captured, spare
-    uint32_t pad[6];
+    cudaTextureObject_t emission;  // the request's volume (0: no gas)
+    cudaTextureObject_t velocity;
+    uint32_t pad[2];
 };
 static_assert(sizeof(ServeRequest) == 256, "ServeRequest");
 
@@ -78,13 +80,12 @@ struct WaveArgs {
     uint32_t flagged_capacity;
     const float* sphere_table;
     const float4* blackbody;
-    cudaTextureObject_t emission;
-    cudaTextureObject_t velocity;
+    uint32_t fp64_all;         // GG_FP64_ALL_FLAGGED
+    uint32_t steps_per_round;  // RK4 steps between refill checks
+    uint32_t refill_idle;      // refill once this many lanes of a warp are idle
 };
 
 constexpr unsigned kFull = 0xffffffffu;
-constexpr int kStepsPerRound = 8;       // RK4 steps between refill checks
-constexpr int kRefillIdle = 8;          // refill once this many lanes are idle
 constexpr uint32_t kMaxRounds = 1u << 28;  // bound on a warp's rounds (each consumes work or a step)
 constexpr uint32_t kMaxFillsPerRound = 64;
 constexpr int kServeThreads = 128;
@@ -121,7 +122,7 @@ __device__ __forceinline__ void account(const WaveArgs& a, bool finished, uint32
 // Write a finished ray, or queue it for FP64 re-integration.
 __device__ __forceinline__ void complete(const WaveArgs& a, uint32_t req, uint32_t pixel, const PixelResult& r) {
     const ServeRequest& R = a.requests[req];
-    if (needs_fp64(R.u, r)) {
+    if (needs_fp64(R.u, r, a.fp64_all != 0u)) {
         uint32_t slot = atomicAdd(&a.header->flagged_count, 1u);
         if (slot < a.flagged_capacity) {
             a.flagged[slot] = ((unsigned long long)req << 32) | pixel;
@@ -140,7 +141,6 @@ __device__ void serve_queue(const WaveArgs& a, uint32_t lane) {
     const ServeChunk* chunks = Kind == 0 ? a.chunks0 : a.chunks1;
     const uint32_t nchunks = a.header->chunk_count[Kind];
     uint32_t* head = &a.header->heads[Kind];
-    const bool gather = a.emission != 0;
     const unsigned lower = (1u << lane) - 1u;
     typename LaneOf<Kind>::type L;
     bool active = false;
@@ -200,20 +200,20 @@ __device__ void serve_queue(const WaveArgs& a, uint32_t lane) {
             continue;
         }
         // Advance every active lane, a few steps per round.
-        for (int it = 0; it < kStepsPerRound; ++it) {
+        for (uint32_t it = 0; it < a.steps_per_round; ++it) {
             bool finished = false;
             PixelResult r{};
             float budget = 0.0f;
             if (active) {
                 const ServeRequest& R = a.requests[req];
                 if constexpr (Kind == 0) {
-                    finished = s_step(L, R.u, a.emission, a.velocity, gather);
+                    finished = s_step(L, R.u, R.emission, R.velocity, R.emission != 0);
                     if (finished) {
                         SweepTables t{a.sphere_table, R.camera_table, R.sky_table};
                         r = s_finish(L, R.u, t, a.blackbody);
                     }
                 } else {
-                    finished = k_step(L, R.u, a.emission, a.velocity, gather);
+                    finished = k_step(L, R.u, R.emission, R.velocity, R.emission != 0);
                     if (finished) r = k_finish(L, R.u, a.blackbody);
                 }
                 budget = R.u.driftBudget;
@@ -225,7 +225,7 @@ __device__ void serve_queue(const WaveArgs& a, uint32_t lane) {
             account(a, finished, req, r, budget, lane);
             act = __ballot_sync(kFull, active);
             if (act == 0u) break;
-            if (!drained && __popc(~act) >= kRefillIdle) break;
+            if (!drained && (uint32_t)__popc(~act) >= a.refill_idle) break;
         }
     }
 }
@@ -249,8 +249,8 @@ __global__ void __launch_bounds__(128) serve_reintegrate_kernel(WaveArgs a) {
         MarchParams p{};
         p.u = R.u;
         p.tables = SweepTables{a.sphere_table, R.camera_table, R.sky_table};
-        p.emission = a.emission;
-        p.velocity = a.velocity;
+        p.emission = R.emission;
+        p.velocity = R.velocity;
         p.blackbody = a.blackbody;
         uint32_t w = R.u.resolution.x;
         PixelResult r = shade_pixel_lane<double>(p, pixel % w, pixel / w);
@@ -372,6 +372,7 @@ struct gg_server {
     bool stop = false;
     int fatal = GG_OK;
     std::string fatal_sentence;
+    int injected = GG_OK;  // gg_server_inject_fault: the next device call "fails" with this status
     std::thread worker;
     uint64_t total_requests = 0, total_steps = 0, total_waves = 0;
     std::vector<std::pair<double, double>> intervals;  // wave device intervals, seconds after `origin`
@@ -403,6 +404,11 @@ static int capture_wave_graph(gg_server* s, WaveSlot& w) {
     cudaGraphDestroy(g);
     GG_CUDA(e, "wave graph instantiate");
     return GG_OK;
+}
+
+// The volume a request marches: its own, or the server's.
+static const gg_volume* request_volume(const gg_server* s, const ServedRequest& r) {
+    return r.q.volume ? r.q.volume : s->vol;
 }
 
 // The per-request baselines: one request at a time through an image kernel.
@@ -486,6 +492,9 @@ static bool form_wave(gg_server* s, WaveSlot& w) {
                 d.color = r.d_color;
                 d.debug = r.d_debug;
                 d.stats = r.d_stats;
+                const gg_volume* vol = request_volume(s, r);
+                d.emission = vol ? vol->emission_tex : 0;
+                d.velocity = vol ? vol->velocity_tex : 0;
                 w.members.push_back(cands[i]);
                 r.waves_pending += 1;
             }
@@ -557,7 +566,7 @@ static int finish_wave(gg_server* s, WaveSlot& w) {
 static int run_plain(gg_server* s, ServedRequest& r) {
     gg_context* ctx = s->ctx;
     GG_CUDA(cudaStreamWaitEvent(s->plain, s->built, 0), "plain ordering");
-    MarchParams p = make_params(ctx, s->vol, r.u, r.q.spin == 0.0f ? &r.sweep : nullptr);
+    MarchParams p = make_params(ctx, request_volume(s, r), r.u, r.q.spin == 0.0f ? &r.sweep : nullptr);
     p.color = r.d_color;
     p.debug = r.d_debug;
     p.target_width = r.q.width;
@@ -665,6 +674,8 @@ static void worker_loop(gg_server* s) {
             }
             ++it;
         }
+        if (status == GG_OK && s->injected != GG_OK)
+            status = fail(s->injected, "Injected fault: the scheduler's device call reported status %d.", s->injected);
         if (status != GG_OK) {
             s->fatal = status;
             s->fatal_sentence = gg_last_error();
@@ -703,6 +714,13 @@ GG_API int gg_server_create(gg_context* ctx, const gg_volume* vol, const gg_serv
     if (s->cfg.mode != GG_SERVE_BATCHED && s->cfg.mode != GG_SERVE_SERIAL_PLAIN &&
         s->cfg.mode != GG_SERVE_SERIAL_PLAIN_AS_WRITTEN)
         return gg::fail(GG_ERR_INVALID_ARGUMENT, "Unknown serving mode %d.", s->cfg.mode);
+    if (s->cfg.steps_per_round == 0) s->cfg.steps_per_round = 8;
+    if (s->cfg.refill_idle == 0) s->cfg.refill_idle = 8;
+    if (s->cfg.steps_per_round > 64 || s->cfg.refill_idle > 32)
+        return gg::fail(GG_ERR_INVALID_ARGUMENT, "steps_per_round %u or refill_idle %u is outside 1..64 / 1..32.",
+                        s->cfg.steps_per_round, s->cfg.refill_idle);
+    if (s->cfg.fp64_policy != GG_FP64_ESCAPING && s->cfg.fp64_policy != GG_FP64_ALL_FLAGGED)
+        return gg::fail(GG_ERR_INVALID_ARGUMENT, "Unknown FP64 policy %u.", s->cfg.fp64_policy);
     if (s->cfg.memory_bytes == 0) s->cfg.memory_bytes = (ctx->budget - ctx->used) / 4;
     if (ctx->used + s->cfg.memory_bytes > ctx->budget)
         return gg::fail(GG_ERR_OVER_BUDGET, "The server asks for %llu bytes but the budget has %llu left.",
@@ -751,8 +769,9 @@ GG_API int gg_server_create(gg_context* ctx, const gg_volume* vol, const gg_serv
         w.args.flagged_capacity = s->flagged_capacity;
         w.args.sphere_table = ctx->sphere_table;
         w.args.blackbody = ctx->blackbody;
-        w.args.emission = vol ? vol->emission_tex : 0;
-        w.args.velocity = vol ? vol->velocity_tex : 0;
+        w.args.fp64_all = s->cfg.fp64_policy == GG_FP64_ALL_FLAGGED ? 1u : 0u;
+        w.args.steps_per_round = s->cfg.steps_per_round;
+        w.args.refill_idle = s->cfg.refill_idle;
         GG_CHECK(gg::capture_wave_graph(s.get(), w));
     }
     GG_CUDA(cudaStreamSynchronize(s->build), "server set-up");
@@ -814,6 +833,8 @@ GG_API int gg_server_submit(gg_server* s, const gg_request* req, uint64_t* ticke
                         (double)VOLUME_HALF_EXTENT);
     if (!(req->fov_y > 0.0f && req->fov_y < 3.1f)) return gg::fail(GG_ERR_INVALID_ARGUMENT, "Field of view %g is invalid.", (double)req->fov_y);
     if (!req->output) return gg::fail(GG_ERR_INVALID_ARGUMENT, "The request has no output buffer.");
+    if (req->volume && req->volume->ctx != s->ctx)
+        return gg::fail(GG_ERR_INVALID_ARGUMENT, "The request's volume belongs to another context.");
     auto r = std::make_shared<gg::ServedRequest>();
     r->q = *req;
     r->u = gg::request_uniforms(*req);
@@ -830,6 +851,16 @@ GG_API int gg_server_submit(gg_server* s, const gg_request* req, uint64_t* ticke
     s->all[r->ticket] = r;
     *ticket = r->ticket;
     s->cv_work.notify_one();
+    return GG_OK;
+}
+
+GG_API int gg_server_inject_fault(gg_server* s, int status) {
+    if (!s || status == GG_OK) return gg::fail(GG_ERR_INVALID_ARGUMENT, "gg_server_inject_fault needs a server and a status.");
+    {
+        std::lock_guard<std::mutex> lock(s->mu);
+        s->injected = status;
+    }
+    s->cv_work.notify_all();
     return GG_OK;
 }
 

@@ -119,7 +119,7 @@ __global__ void __launch_bounds__(256) bin_kernel(SplatArgs a) {
     const uint32_t n = u.volumeSize;
     for_each_corner(f, u, a.first_index + i, [&](int x, int y, int z, float w) {
         Deposit d = deposit_values(w, f.energy, f.relative, v.x, v.y, v.z);
-        uint32_t* rec = a.sums + 6u * (((uint32_t)z * n + (uint32_t)y) * n + (uint32_t)x);
+        uint32_t* rec = a.sums + 6ull * (((uint32_t)z * n + (uint32_t)y) * n + (uint32_t)x);
 #pragma unroll
         for (int k = 0; k < 6; ++k) atomicAdd(rec + k, d.w[k]);
     });
@@ -293,7 +293,7 @@ __global__ void __launch_bounds__(kBrickBlock) brick_deposit_kernel(BrickArgs a)
         const uint32_t cell = w / 6u, c = w - cell * 6u;
         const uint32_t tx = cell % T, ty = (cell / T) % T, tz = cell / (T * T);
         const uint32_t x = (uint32_t)ox + tx, y = (uint32_t)oy + ty, z = (uint32_t)oz + tz;
-        if (x < n && y < n && z < n) atomicAdd(a.sums + 6u * ((z * n + y) * n + x) + c, val);
+        if (x < n && y < n && z < n) atomicAdd(a.sums + 6ull * ((z * n + y) * n + x) + c, val);
     }
 }
 
@@ -305,33 +305,32 @@ struct ResolveArgs {
     cudaSurfaceObject_t velocity;
     const float4* __restrict__ blackbody;
     SplatUniforms u;
+    double log_t_min, log_t_max;  // gg_log_d of the blackbody range, the same values on every device and host
 };
 
 // Blackbody coordinate (Common.h:56-59) in double with the shared series
 // log, rounded once, so the resolve's bits match the CPU replica's.
-__device__ __forceinline__ float bb_coordinate_det(float temperature) {
+__device__ __forceinline__ float bb_coordinate_det(float temperature, double lo, double hi) {
     float t = fminf(fmaxf(temperature, BLACKBODY_T_MIN), BLACKBODY_T_MAX);
-    double lo = gg_log_d((double)BLACKBODY_T_MIN);
-    double hi = gg_log_d((double)BLACKBODY_T_MAX);
     return (float)((gg_log_d((double)t) - lo) / (hi - lo));
 }
 
 // resolveVolume (splat.metal:93-120) fused with the clear of the sums
 // (Volume.swift:34-43): each voxel's record is read once and written back
-// as zeros.
-__global__ void __launch_bounds__(256) resolve_kernel(ResolveArgs a) {
+// as zeros. Grid: x along blocks of kResolveBlock threads, y and z in the
+// grid's y and z (no index divisions).
+constexpr uint32_t kResolveBlock = 128;
+
+__global__ void __launch_bounds__(kResolveBlock) resolve_kernel(ResolveArgs a) {
     const uint32_t n = a.u.volumeSize;
-    const uint64_t total = (uint64_t)n * n * n;
-    uint64_t index = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (index >= total) return;
-    uint2* rec = reinterpret_cast<uint2*>(a.sums + 6u * index);
+    const uint32_t x = blockIdx.x * blockDim.x + threadIdx.x, y = blockIdx.y, z = blockIdx.z;
+    if (x >= n) return;
+    const uint32_t index = (z * n + y) * n + x;
+    uint2* rec = reinterpret_cast<uint2*>(a.sums + 6ull * index);
     uint2 r0 = rec[0], r1 = rec[1], r2 = rec[2];
     rec[0] = make_uint2(0u, 0u);
     rec[1] = make_uint2(0u, 0u);
     rec[2] = make_uint2(0u, 0u);
-    uint32_t x = (uint32_t)(index % n);
-    uint32_t y = (uint32_t)((index / n) % n);
-    uint32_t z = (uint32_t)(index / ((uint64_t)n * n));
     float voxel = 2.0f * a.u.halfExtent / (float)n;
     float inverse_volume = 1.0f / (voxel * voxel * voxel);
     float count = (float)r2.y / MASS_FIXED;
@@ -340,7 +339,7 @@ __global__ void __launch_bounds__(256) resolve_kernel(ResolveArgs a) {
     float tr = 0.0f, tg = 0.0f, tb = 0.0f;
     if (energy > 0.0f) {
         float mean_t = energy_t / energy * a.u.peakTemperature;
-        float c = bb_coordinate_det(mean_t) * (float)BLACKBODY_TABLE_SIZE - 0.5f;
+        float c = bb_coordinate_det(mean_t, a.log_t_min, a.log_t_max) * (float)BLACKBODY_TABLE_SIZE - 0.5f;
         float fl = floorf(c);
         float f = c - fl;
         int i0 = (int)fl, i1 = i0 + 1;
@@ -627,9 +626,10 @@ GG_API int gg_splat_resolve(gg_volume* vol, const SplatUniforms* u, const gg_par
     gg_context* ctx = vol->ctx;
     std::lock_guard<std::recursive_mutex> lock(ctx->mu);
     GG_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
-    ResolveArgs a{vol->sums, vol->emission_surf, vol->velocity_surf, ctx->blackbody, *u};
-    const uint64_t total = (uint64_t)vol->size * vol->size * vol->size;
-    resolve_kernel<<<(unsigned)((total + 255u) / 256u), 256, 0, ctx->stream>>>(a);
+    ResolveArgs a{vol->sums, vol->emission_surf, vol->velocity_surf, ctx->blackbody, *u,
+                  gg_log_d((double)BLACKBODY_T_MIN), gg_log_d((double)BLACKBODY_T_MAX)};
+    const uint32_t n = vol->size;
+    resolve_kernel<<<dim3((n + kResolveBlock - 1u) / kResolveBlock, n, n), kResolveBlock, 0, ctx->stream>>>(a);
     return gg::launch_status("splat resolve");
 }
 

@@ -260,6 +260,10 @@ class Context:
                                         C.byref(t)))
         return t.value
 
+    def set_fp64_policy(self, policy: int):
+        """gg_context_set_fp64_policy for gg_march and gg_probe."""
+        check(lib().gg_context_set_fp64_policy(self.handle, policy))
+
     def fp32_peak_tflops(self) -> float:
         t = C.c_double()
         check(lib().gg_measure_fp32_peak(self.handle, C.byref(t)))
@@ -595,6 +599,7 @@ class RequestSpec:
     fov_y: float = 50.0 * math.pi / 180.0
     star_seed: int = 1
     flags: int = 0
+    volume: "Volume | None" = None  # None: the server's volume
 
 
 class Server:
@@ -602,10 +607,12 @@ class Server:
     per-request baseline (SERVE_SERIAL_PLAIN) over one resident volume."""
 
     def __init__(self, ctx: Context, vol: Volume | None, mode: int = T.SERVE_BATCHED, memory_bytes: int = 0,
-                 wave_rays: int = 0, chunk_rays: int = 0, max_waves_in_flight: int = 0):
+                 wave_rays: int = 0, chunk_rays: int = 0, max_waves_in_flight: int = 0,
+                 fp64_policy: int = T.FP64_ESCAPING, steps_per_round: int = 0, refill_idle: int = 0):
         self.ctx = ctx
         self.handle = C.c_void_p()
-        cfg = T.ServerConfig(mode, memory_bytes, wave_rays, chunk_rays, max_waves_in_flight)
+        cfg = T.ServerConfig(mode, memory_bytes, wave_rays, chunk_rays, max_waves_in_flight, fp64_policy,
+                             steps_per_round, refill_idle)
         check(lib().gg_server_create(ctx.handle, vol.handle if vol else None, C.byref(cfg), C.byref(self.handle)))
         ctx.adopt(self)
         self._buffers = {}
@@ -631,7 +638,8 @@ class Server:
         dbg = np.zeros((n, 4), np.float16) if debug else None
         q = T.Request(spec.azimuth, spec.elevation, spec.distance, spec.fov_y, spec.width, spec.height,
                       spec.step_cap, spec.spin, spec.star_seed & 0xFFFFFFFF, spec.flags,
-                      output.ctypes.data, dbg.ctypes.data if dbg is not None else None)
+                      output.ctypes.data, dbg.ctypes.data if dbg is not None else None,
+                      spec.volume.handle if spec.volume is not None else None)
         t = C.c_uint64()
         check(lib().gg_server_submit(self.handle, C.byref(q), C.byref(t)))
         self._buffers[t.value] = (output, dbg)
@@ -655,3 +663,43 @@ class Server:
                                      C.byref(e)))
         return {"requests": a.value, "ray_steps": b.value, "launches": c.value, "busy_seconds": d.value,
                 "span_seconds": e.value}
+
+
+class Sequence:
+    """A sequence render request (the still's --sequence frames,
+    Still.swift:67-90) served alongside other requests: its own particle
+    system advances one dispatch and splats stochastically into its own
+    volume before each frame, and each frame is an interactive 256-step
+    request on `server` marching that volume. Frames run in order: frame
+    k + 1's splat waits until frame k's rays are done with the volume."""
+
+    def __init__(self, server: "Server", ctx: Context, particles: int, size: int, frames: int, width: int = 960,
+                 height: int = 540, spin: float = 0.0, seed: int = 1, camera: OrbitCamera | None = None,
+                 settle_dispatches: int = 300):
+        self.server = server
+        self.frames = frames
+        self.camera = camera or OrbitCamera()
+        self.width, self.height, self.spin, self.seed = width, height, spin, seed
+        self.particles = Particles(ctx, particles, seed)
+        self.particles.advance(settle_dispatches, seed_first=True)
+        self.volume = Volume(ctx, size)
+
+    def spec(self) -> RequestSpec:
+        c = self.camera
+        return RequestSpec(self.width, self.height, 256, self.spin, c.azimuth, c.elevation, c.distance, c.fov_y,
+                           star_seed=self.seed & 0xFFFFFFFF, volume=self.volume)
+
+    def frame(self, timeout_s: float = 600.0):
+        """Advance, splat, serve one frame: (pixels, RequestResult)."""
+        self.particles.step(1)
+        self.volume.splat(self.particles, exact=False)
+        pixels, _, res = self.server.wait(self.server.submit(self.spec()), timeout_s)
+        return pixels, res
+
+    def run(self):
+        return [self.frame() for _ in range(self.frames)]
+
+    def close(self):
+        self.volume.close()
+        self.particles.close()
+

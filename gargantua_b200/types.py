@@ -139,7 +139,7 @@ class Request(C.Structure):
     _fields_ = [
         ("azimuth", f32), ("elevation", f32), ("distance", f32), ("fov_y", f32),
         ("width", u32), ("height", u32), ("step_cap", u32), ("spin", f32), ("star_seed", u32), ("flags", u32),
-        ("output", C.c_void_p), ("debug_output", C.c_void_p),
+        ("output", C.c_void_p), ("debug_output", C.c_void_p), ("volume", C.c_void_p),
     ]
 
 
@@ -153,9 +153,10 @@ class RequestResult(C.Structure):
 
 class ServerConfig(C.Structure):
     _fields_ = [("mode", C.c_int), ("memory_bytes", C.c_uint64), ("wave_rays", u32), ("chunk_rays", u32),
-                ("max_waves_in_flight", u32)]
+                ("max_waves_in_flight", u32), ("fp64_policy", u32), ("steps_per_round", u32), ("refill_idle", u32)]
 
 
+FP64_ESCAPING, FP64_ALL_FLAGGED = 0, 1
 SERVE_BATCHED, SERVE_SERIAL_PLAIN, SERVE_SERIAL_PLAIN_AS_WRITTEN = 0, 1, 2
 REQUEST_NO_STARS, REQUEST_NO_REDSHIFT = 1, 2
 

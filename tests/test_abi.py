@@ -109,3 +109,35 @@ def test_context_without_a_device_reports_no_device():
         g.Context()
     assert e.value.status == 7  # GG_ERR_NO_DEVICE
     assert "device" in e.value.sentence.lower()
+
+
+def test_library_structs_match_their_ctypes_mirrors(tmp_path):
+    """gg_request, gg_request_result and gg_server_config (this library's own
+    structs) have the sizes and offsets the Python mirrors assume."""
+    import subprocess
+
+    from gargantua_b200 import types as T
+
+    checks = {
+        "gg_request": (T.Request, ["azimuth", "width", "flags", "output", "debug_output", "volume"]),
+        "gg_request_result": (T.RequestResult, ["submitted", "ray_steps", "counters", "status"]),
+        "gg_server_config": (T.ServerConfig, ["mode", "memory_bytes", "wave_rays", "max_waves_in_flight",
+                                             "fp64_policy", "steps_per_round", "refill_idle"]),
+    }
+    lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "gargantua.h"', "int main(void){"]
+    for cname, (_, fields) in checks.items():
+        lines.append(f'printf("{cname} %zu\\n", sizeof({cname}));')
+        for f in fields:
+            lines.append(f'printf("{cname}.{f} %zu\\n", offsetof({cname}, {f}));')
+    lines.append("return 0;}")
+    src = tmp_path / "s.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "s"
+    r = subprocess.run(["/usr/bin/gcc", "-std=c11", str(src), "-I", os.path.join(ROOT, "include"), "-o", str(exe)],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    got = dict(line.split() for line in subprocess.run([str(exe)], capture_output=True, text=True).stdout.splitlines())
+    for cname, (struct, fields) in checks.items():
+        assert int(got[cname]) == C.sizeof(struct), cname
+        for f in fields:
+            assert int(got[f"{cname}.{f}"]) == getattr(struct, f).offset, f"{cname}.{f}"

@@ -146,11 +146,68 @@ def test_server_autotune_picks_a_measured_candidate(world):
 
     specs = mix_specs()[:4]
     tuned = autotune.tune_server(world["ctx"], world["vol"], specs, chunks=(32, 64), waves=(1 << 20,),
-                                 in_flight=(2,), repeats=1)
+                                 in_flight=(2,), cadences=((8, 8), (4, 4)), repeats=1)
     assert tuned["chunk_rays"] in (32, 64) and tuned["rate"] > 0.0
-    assert len(tuned["trials"]) == 2 and max(t["rate"] for t in tuned["trials"]) == tuned["rate"]
-    server = g.Server(world["ctx"], world["vol"], g.types.SERVE_BATCHED, chunk_rays=tuned["chunk_rays"],
-                      wave_rays=tuned["wave_rays"], max_waves_in_flight=tuned["max_waves_in_flight"])
+    assert (tuned["steps_per_round"], tuned["refill_idle"]) in ((8, 8), (4, 4))
+    assert len(tuned["trials"]) == 5
+    shape = {k: tuned[k] for k in ("chunk_rays", "wave_rays", "max_waves_in_flight", "steps_per_round", "refill_idle")}
+    server = g.Server(world["ctx"], world["vol"], g.types.SERVE_BATCHED, **shape)
     pixels, _, res = server.wait(server.submit(specs[0]))
     assert res.status == 0 and res.counters.rays == specs[0].width * specs[0].height
     server.close()
+
+
+def test_sequence_frames_march_their_own_advancing_volume(world):
+    """Sequence frames served in a mix with a still: each frame equals the
+    plain march of the same sim state within the served-vs-plain bar, and
+    the frames change as the disk advances."""
+    import gargantua_b200 as g
+
+    ctx = world["ctx"]
+    server = g.Server(ctx, world["vol"], g.types.SERVE_BATCHED)
+    seq = g.Sequence(server, ctx, 50_000, 48, frames=3, width=320, height=180, spin=0.0, seed=4,
+                     settle_dispatches=50)
+    # A replica of the sequence's state, marched per frame with gg_march.
+    ps = g.Particles(ctx, 50_000, seed=4)
+    ps.advance(50, seed_first=True)
+    vol = g.Volume(ctx, 48)
+    t = g.Targets(ctx, 320, 180)
+    other = server.submit(g.RequestSpec(640, 360, 4096, 0.9))
+    lums = []
+    for k in range(3):
+        pixels, res = seq.frame()
+        assert res.status == 0 and res.counters.rays == 320 * 180
+        ps.step(1)
+        vol.splat(ps, exact=False)
+        u = g.uniforms(seq.camera, 320, 180, g.Settings.interactive(), 1e-4, True, 4)
+        ctx.enable_tables(u, float(np.float32(seq.camera.distance)))
+        g.march(ctx, vol, u, t)
+        ref, _, _ = t.read()
+        la, lb = luminance(pixels), luminance(ref)
+        assert np.abs(la - lb).sum() / max(lb.sum(), 1e-30) < 1e-2, k
+        lums.append(la)
+    assert not np.array_equal(lums[0], lums[2])  # the disk moved
+    server.wait(other)
+    t.close()
+    vol.close()
+    ps.close()
+    seq.close()
+    server.close()
+
+
+def test_fp64_policy_skips_captured_rays_by_default(world):
+    """GG_FP64_ESCAPING re-integrates fewer rays than GG_FP64_ALL_FLAGGED on
+    a Kerr still whose flagged rays are mostly captured; the images agree."""
+    import gargantua_b200 as g
+
+    spec = g.RequestSpec(480, 270, 4096, 0.9, azimuth=1.0, elevation=0.4, distance=52.0)
+    counts, lum = {}, {}
+    for policy in (g.types.FP64_ESCAPING, g.types.FP64_ALL_FLAGGED):
+        server = g.Server(world["ctx"], world["vol"], g.types.SERVE_BATCHED, fp64_policy=policy)
+        (pix, _, res), = run(server, [spec])
+        counts[policy] = int(res.fp64_rays)
+        lum[policy] = luminance(pix)
+        server.close()
+    assert counts[g.types.FP64_ALL_FLAGGED] > counts[g.types.FP64_ESCAPING]
+    a, b = lum[g.types.FP64_ESCAPING], lum[g.types.FP64_ALL_FLAGGED]
+    assert np.abs(a - b).sum() / max(b.sum(), 1e-30) < 1e-3
