@@ -135,7 +135,7 @@ struct gg_volume {
     // (0: direct global atomics) and particles per deposit work item.
     uint32_t brick_edge[2] = {8u, 8u};
     uint32_t brick_chunk[2] = {4096u, 2048u};
-    void* brick_scratch = nullptr;  // counts, offsets, cursor, items, sorted slots
+    void* brick_scratch = nullptr;  // counts, offsets, cursor, items, sorted slots, keys
     uint64_t brick_scratch_capacity = 0;
 };
 

@@ -129,13 +129,13 @@ __global__ void __launch_bounds__(256) bin_kernel(SplatArgs a) {
 // Brick-privatised splat. The grid is cut into bricks of B^3 voxels; a
 // particle belongs to the brick holding its low corner, so its eight corners
 // fall in that brick's (B+1)^3 tile. Four launches:
-//   count    per-block shared histogram of particles per brick, summed into
-//            global counts;
+//   count    each particle's brick (its key, stored) and a per-block shared
+//            histogram of keys, summed into global counts;
 //   scan     one block: brick offsets and work items (ceil(count / chunk)
 //            particles-chunks per brick);
-//   scatter  the same histogram again, each block reserving its range of
-//            every brick with one atomic, then particle indices written into
-//            brick order;
+//   scatter  the histogram again from the stored keys, each block reserving
+//            its range of every brick with one atomic, then particle indices
+//            written into brick order;
 //   deposit  one block per work item: the tile's six-word records zeroed in
 //            shared memory, the chunk's particles deposited there with
 //            shared atomics, the non-zero words added to the sums with one
@@ -144,7 +144,8 @@ __global__ void __launch_bounds__(256) bin_kernel(SplatArgs a) {
 // the direct kernel's bit for bit.
 
 constexpr uint32_t kBrickBlock = 256;
-constexpr uint32_t kBrickParticlesPerBlock = 8192;  // count/scatter range of one block
+constexpr uint32_t kBrickParticlesPerBlock = 2048;  // count/scatter range of one block
+constexpr uint32_t kOutside = 0xFFFFFFFFu;          // key of a particle outside the cube
 constexpr uint32_t kMaxBricks = 32768;               // histogram of 128 KB shared memory
 
 struct BrickArgs {
@@ -162,6 +163,7 @@ struct BrickArgs {
     uint32_t* cursor;    // [bricks], reservation cursor
     uint32_t* items;     // [bricks + 1], exclusive scan of ceil(count / chunk)
     uint32_t* sorted;    // [particleCount], particle slots in brick order
+    uint32_t* keys;      // [particleCount], each particle's brick (kOutside: none), from the count pass
 };
 
 __device__ __forceinline__ uint32_t brick_of(const Footprint& f, const BrickArgs& a) {
@@ -176,7 +178,12 @@ __global__ void __launch_bounds__(kBrickBlock) brick_count_kernel(BrickArgs a) {
     const uint32_t end = min(begin + kBrickParticlesPerBlock, a.u.particleCount);
     for (uint32_t i = begin + threadIdx.x; i < end; i += blockDim.x) {
         Footprint f;
-        if (footprint(a.pos[i], a.u, f)) atomicAdd(&hist[brick_of(f, a)], 1u);
+        uint32_t key = kOutside;
+        if (footprint(a.pos[i], a.u, f)) {
+            key = brick_of(f, a);
+            atomicAdd(&hist[key], 1u);
+        }
+        a.keys[i] = key;
     }
     __syncthreads();
     for (uint32_t b = threadIdx.x; b < a.bricks; b += blockDim.x)
@@ -227,8 +234,8 @@ __global__ void __launch_bounds__(kBrickBlock) brick_scatter_kernel(BrickArgs a)
     const uint32_t begin = blockIdx.x * kBrickParticlesPerBlock;
     const uint32_t end = min(begin + kBrickParticlesPerBlock, a.u.particleCount);
     for (uint32_t i = begin + threadIdx.x; i < end; i += blockDim.x) {
-        Footprint f;
-        if (footprint(a.pos[i], a.u, f)) atomicAdd(&hist[brick_of(f, a)], 1u);
+        const uint32_t key = a.keys[i];
+        if (key < a.bricks) atomicAdd(&hist[key], 1u);
     }
     __syncthreads();
     // This block's range of every brick it touches, then a shared cursor.
@@ -236,10 +243,10 @@ __global__ void __launch_bounds__(kBrickBlock) brick_scatter_kernel(BrickArgs a)
         if (hist[b]) hist[b] = atomicAdd(&a.cursor[b], hist[b]);
     __syncthreads();
     for (uint32_t i = begin + threadIdx.x; i < end; i += blockDim.x) {
-        Footprint f;
-        if (!footprint(a.pos[i], a.u, f)) continue;
-        const uint32_t slot = atomicAdd(&hist[brick_of(f, a)], 1u);
-        if (slot < a.u.particleCount) a.sorted[slot] = i;  // always: the count pass saw the same particles
+        const uint32_t key = a.keys[i];
+        if (key >= a.bricks) continue;
+        const uint32_t slot = atomicAdd(&hist[key], 1u);
+        if (slot < a.u.particleCount) a.sorted[slot] = i;  // always: the counts came from the same keys
     }
 }
 
@@ -423,7 +430,7 @@ static int splat_bin_shaped(gg_particles* ps, gg_volume* vol, const SplatUniform
     const uint32_t per = bricks_per_axis(vol->size, edge);
     const uint32_t bricks = per * per * per;
     const uint64_t words = align256(4ull * bricks) * 2u + align256(4ull * (bricks + 1u)) * 2u;
-    const uint64_t bytes = words + align256(4ull * ps->count);
+    const uint64_t bytes = words + 2u * align256(4ull * ps->count);
     GG_CHECK(gg::ensure_capacity(ctx, &vol->brick_scratch, &vol->brick_scratch_capacity, bytes, "splat bricks"));
     char* base = static_cast<char*>(vol->brick_scratch);
     BrickArgs a;
@@ -441,6 +448,7 @@ static int splat_bin_shaped(gg_particles* ps, gg_volume* vol, const SplatUniform
     a.offsets = reinterpret_cast<uint32_t*>(base + 2u * align256(4ull * bricks));
     a.items = reinterpret_cast<uint32_t*>(base + 2u * align256(4ull * bricks) + align256(4ull * (bricks + 1u)));
     a.sorted = reinterpret_cast<uint32_t*>(base + words);
+    a.keys = reinterpret_cast<uint32_t*>(base + words + align256(4ull * ps->count));
     GG_CUDA(cudaMemsetAsync(a.counts, 0, 4ull * bricks, ctx->stream), "brick counts");
     const int hist = (int)(4u * bricks);
     GG_CHECK(allow_shared((const void*)brick_count_kernel, hist, ctx->device, 0));
