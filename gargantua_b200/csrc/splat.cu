@@ -190,40 +190,55 @@ __global__ void __launch_bounds__(kBrickBlock) brick_count_kernel(BrickArgs a) {
         if (hist[b]) atomicAdd(&a.counts[b], hist[b]);
 }
 
-// One block of 1024 threads: each thread scans a contiguous run of bricks.
+// Inclusive sum over the warp of a value per lane (shuffle scan).
+__device__ __forceinline__ uint32_t warp_inclusive(uint32_t v, uint32_t lane) {
+#pragma unroll
+    for (uint32_t off = 1; off < 32u; off <<= 1) {
+        uint32_t u = __shfl_up_sync(0xffffffffu, v, off);
+        if (lane >= off) v += u;
+    }
+    return v;
+}
+
+// One block of 1024 threads: each thread scans a contiguous run of bricks;
+// the per-thread totals are scanned with warp shuffles and one pass over the
+// 32 warp totals.
 __global__ void __launch_bounds__(1024) brick_scan_kernel(BrickArgs a) {
-    __shared__ uint32_t part_p[1024], part_i[1024];
+    __shared__ uint32_t warp_p[32], warp_i[32];
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
     const uint32_t per = (a.bricks + blockDim.x - 1) / blockDim.x;
     const uint32_t b0 = threadIdx.x * per, b1 = min(b0 + per, a.bricks);
     uint32_t sp = 0, si = 0;
     for (uint32_t b = b0; b < b1; ++b) {
-        sp += a.counts[b];
-        si += (a.counts[b] + a.chunk - 1u) / a.chunk;
+        const uint32_t c = a.counts[b];
+        sp += c;
+        si += (c + a.chunk - 1u) / a.chunk;
     }
-    part_p[threadIdx.x] = sp;
-    part_i[threadIdx.x] = si;
+    const uint32_t ip = warp_inclusive(sp, lane), ii = warp_inclusive(si, lane);
+    if (lane == 31u) {
+        warp_p[warp] = ip;
+        warp_i[warp] = ii;
+    }
     __syncthreads();
-    // Hillis-Steele inclusive scan of the per-thread totals.
-    for (uint32_t off = 1; off < blockDim.x; off <<= 1) {
-        uint32_t vp = threadIdx.x >= off ? part_p[threadIdx.x - off] : 0u;
-        uint32_t vi = threadIdx.x >= off ? part_i[threadIdx.x - off] : 0u;
-        __syncthreads();
-        part_p[threadIdx.x] += vp;
-        part_i[threadIdx.x] += vi;
-        __syncthreads();
+    if (warp == 0) {
+        const uint32_t wp = warp_inclusive(warp_p[lane], lane), wi = warp_inclusive(warp_i[lane], lane);
+        warp_p[lane] = wp;  // inclusive totals through warp `lane`
+        warp_i[lane] = wi;
     }
-    uint32_t op = threadIdx.x ? part_p[threadIdx.x - 1] : 0u;
-    uint32_t oi = threadIdx.x ? part_i[threadIdx.x - 1] : 0u;
+    __syncthreads();
+    uint32_t op = (warp ? warp_p[warp - 1] : 0u) + ip - sp;  // exclusive prefix of this thread's run
+    uint32_t oi = (warp ? warp_i[warp - 1] : 0u) + ii - si;
     for (uint32_t b = b0; b < b1; ++b) {
+        const uint32_t c = a.counts[b];
         a.offsets[b] = op;
         a.cursor[b] = op;
         a.items[b] = oi;
-        op += a.counts[b];
-        oi += (a.counts[b] + a.chunk - 1u) / a.chunk;
+        op += c;
+        oi += (c + a.chunk - 1u) / a.chunk;
     }
     if (threadIdx.x == blockDim.x - 1) {
-        a.offsets[a.bricks] = part_p[blockDim.x - 1];
-        a.items[a.bricks] = part_i[blockDim.x - 1];
+        a.offsets[a.bricks] = warp_p[31];
+        a.items[a.bricks] = warp_i[31];
     }
 }
 
