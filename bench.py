@@ -56,6 +56,9 @@ STREAM_LENGTH = 512
 FLOPS_SCHWARZSCHILD_STEP = 192  # RK4 165 + position 14 + step policy 3 + path 10
 FLOPS_KERR_STEP = 515           # RK4 436 + step policy, position, path, Carter and null gauges 79
 FLOPS_SAMPLE = 111              # in-slab gather 67 + static-observer direction 44
+# DRAM bytes of one serve_kerr_kernel launch (ncu, 1920x1080 4096-step Kerr still): the march
+# reads only its descriptors and tables from HBM; pixels stay in L2 until the copy-out.
+SERVE_KERR_TRAFFIC_BYTES = 8408320
 
 
 def make_stream(seed: int, count: int = STREAM_LENGTH):
@@ -530,17 +533,24 @@ def main():
         server_plain = g.Server(ctx, vol, mode)
         serve_slice(server_plain, slices[0], pinned_outputs(slices[0]))
         barrier()
+        sampler = ClockSampler(local)
+        sampler.start()
         p_span = p_wall = p_steps = 0.0
+        per_step = []
         for s, pin in zip(timed, pins):
             results, w, sp, bu, la = serve_slice(server_plain, s, pin)
+            steps = sum(r.ray_steps for r in results)
             p_span += sp
             p_wall += w
-            p_steps += sum(r.ray_steps for r in results)
+            p_steps += steps
+            per_step.append(steps / max(sp, 1e-12))
         barrier()
+        p_clocks = sampler.stop()
         p_span, p_wall, p_steps = max_over_ranks(p_span), max_over_ranks(p_wall), sum_over_ranks(p_steps)
         out = {"value": p_steps / p_span, "e2e": p_steps / p_wall, "unit": "ray-steps/s",
                "served_over_plain": value / (p_steps / p_span),
-               "served_over_plain_e2e": e2e / (p_steps / p_wall)}
+               "served_over_plain_e2e": e2e / (p_steps / p_wall),
+               "per_step_values": per_step, "clocks": p_clocks}
         lat = stream[nslices * B:nslices * B + args.latency_requests]
         if len(lat) >= 8:
             out["p50_ms"], out["p99_ms"] = latency_replay(server_plain, lat)
@@ -596,9 +606,12 @@ def main():
         "e2e": {"value": e2e, "unit": "ray-steps/s", "h2d_bytes_per_step": int(B * 64),
                 "d2h_bytes_per_step": int(d2h / max(args.steps, 1))},
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
-                     "frac": achieved / peak, "traffic": None,
+                     "frac": achieved / peak, "traffic": SERVE_KERR_TRAFFIC_BYTES,
+                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one serve_kerr_kernel "
+                                       "launch serving a 1920x1080 4096-step Kerr still",
                      "peak_source": "measured FP32 FMA microbenchmark (gg_measure_fp32_peak) on this GPU",
-                     "kernel": "serve_kernel (persistent, work-stealing)"},
+                     "kernel": "serve_kerr_kernel + serve_schwarzschild_kernel (persistent, work-stealing)",
+                     "device_busy_fraction": busy / max(span, 1e-12)},
         "cpu_baseline": cpu,
         "passes": passes,
         "clocks": clock_info,

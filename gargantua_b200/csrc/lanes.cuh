@@ -406,11 +406,14 @@ template <typename R> __device__ __forceinline__ void k_sin_inverses(R st, R* in
 template <typename R> __device__ __forceinline__ R k_sin2(R st) { return gmax(st * st, R(sizeof(R) == 4 ? 1e-8 : 1e-12)); }
 
 // Hamilton's equations with the off-shell Sigma terms (Kerr.h:63-90), at a
-// polar angle whose sine and cosine are given. Also returns F = 2 Sigma H,
-// the null residual of the state (Kerr.h:44-50), and 1/sin^2.
+// polar angle whose sine and cosine are given, returned as Sigma times the
+// derivative (every component carries the factor 1/Sigma, which the caller
+// folds into its RK4 weights) with 1/Sigma in *inv_sigma_out. Also returns
+// F = 2 Sigma H, the null residual of the state (Kerr.h:44-50), and
+// 1/sin^2.
 template <typename R>
 __device__ __forceinline__ KState<R> k_derivative(const KConst<R>& k, const KState<R>& s, R st, R ct, R* F_out,
-                                                  R* inv_sin2_out) {
+                                                  R* inv_sin2_out, R* inv_sigma_out) {
     const R r = s.r;
     const R r2 = r * r;
     const R delta = fmaT(r, r - R(2), k.a2);  // r^2 - 2r + a^2
@@ -433,12 +436,13 @@ __device__ __forceinline__ KState<R> k_derivative(const KConst<R>& k, const KSta
     const R two_h = F * inv_sigma;
     const R dprime = fmaT(R(2), r, R(-2));
     const R fr = fmaT(dprime, pr2, inv_delta * fmaT(p2d, dprime, -k.four_E * r * p));
+    *inv_sigma_out = inv_sigma;
     KState<R> o;
-    o.r = delta * s.pr * inv_sigma;
-    o.th = s.pt * inv_sigma;
-    o.ph = (fmaT(k.a, p * inv_delta, k.L * inv_sin2) - k.aE) * inv_sigma;
-    o.pr = fmaT(r, two_h, R(-0.5) * fr) * inv_sigma;
-    o.pt = -ct * fmaT(k.a2 * st, two_h, fmaT(k.a2E2, st, -k.L2 * inv_sin2 * inv_sc)) * inv_sigma;
+    o.r = delta * s.pr;
+    o.th = s.pt;
+    o.ph = fmaT(k.a, p * inv_delta, k.L * inv_sin2) - k.aE;
+    o.pr = fmaT(r, two_h, R(-0.5) * fr);
+    o.pt = -ct * fmaT(k.a2 * st, two_h, fmaT(k.a2E2, st, -k.L2 * inv_sin2 * inv_sc));
     return o;
 }
 
@@ -497,13 +501,13 @@ __device__ __forceinline__ KState<R> k_increment(const KConst<R>& k, const KStat
                 fast_sincos(x.th, &st, &ct);
             }
         }
-        R F, inv_sin2;
-        KState<R> d = k_derivative(k, x, st, ct, &F, &inv_sin2);
+        R F, inv_sin2, inv_sigma;
+        KState<R> d = k_derivative(k, x, st, ct, &F, &inv_sin2, &inv_sigma);  // Sigma times the derivative
         if (stage == 0 && gauged) *gauge = gmax(*gauge, k_gauge(k, s, ct, F, inv_sin2, carter0));
         R wk = (stage == 0 || stage == 3) ? R(1) : R(2);
-        acc = k_offset(acc, d, wk);
+        acc = k_offset(acc, d, wk * inv_sigma);
         if (stage == 3) break;
-        const R wx = stage < 2 ? R(0.5) * h : h;
+        const R wx = (stage < 2 ? R(0.5) * h : h) * inv_sigma;
         x = k_offset(s, d, wx);
         shift = d.th * wx;
     }
