@@ -490,12 +490,14 @@ def main():
     d2h = 0
     schw_requests = 0
     drift_over = rays_total = 0
+    served_per_step = []
     for s, pin in zip(timed, pins):
         results, w, sp, bu, la = serve_slice(batched, s, pin)
         wall += w
         span += sp
         busy += bu
         launches += la
+        served_per_step.append(sum(r.ray_steps for r in results) / max(sp, 1e-12))
         for q, r in zip(s, results):
             steps_total += r.ray_steps
             flops_total += flops_of(q, r)
@@ -600,6 +602,7 @@ def main():
                    "l2": "inputs larger than L2 (outputs up to 66 MB per request, 8-200 MB per step)"},
         "p50_ms": p50,
         "p99_ms": p99,
+        "per_step_values": served_per_step,
         "plain_per_request": plain,
         "plain_lane_per_request": plain_lane,
         "drift": {"rays": rays_total, "over_budget": drift_over, "vs_fp64_oracle": drift_oracle},
