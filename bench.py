@@ -458,6 +458,7 @@ def main():
     stream = make_stream(1 + rank)
     slices = [stream[i * B:(i + 1) * B] for i in range(nslices)]
     shape = {"chunk_rays": 32, "wave_rays": 4 << 20, "max_waves_in_flight": 2, "steps_per_round": 8, "refill_idle": 8,
+             "schedule": 0,
              "chosen_by": "defaults"}
     if not args.no_tune:
         # Untimed: the server's wave shape from a sample of other requests
@@ -467,7 +468,7 @@ def main():
         sample = [spec_of(q) for q in make_stream(1000 + rank)[:16]]
         tuned = autotune.tune_server(ctx, vol, sample)
         shape = {k: tuned[k] for k in ("chunk_rays", "wave_rays", "max_waves_in_flight", "steps_per_round",
-                                         "refill_idle")}
+                                         "refill_idle", "schedule")}
         shape["chosen_by"] = "gargantua_b200.autotune.tune_server on 16 requests of stream seed 1000"
     batched = g.Server(ctx, vol, g.types.SERVE_BATCHED,
                        **{k: v for k, v in shape.items() if k != "chosen_by"})
@@ -552,7 +553,9 @@ def main():
         out = {"value": p_steps / p_span, "e2e": p_steps / p_wall, "unit": "ray-steps/s",
                "served_over_plain": value / (p_steps / p_span),
                "served_over_plain_e2e": e2e / (p_steps / p_wall),
-               "per_step_values": per_step, "clocks": p_clocks}
+               "per_step_values": per_step, "clocks": p_clocks,
+               "median_step_value": statistics.median(per_step),
+               "served_over_plain_median": statistics.median(served_per_step) / statistics.median(per_step)}
         lat = stream[nslices * B:nslices * B + args.latency_requests]
         if len(lat) >= 8:
             out["p50_ms"], out["p99_ms"] = latency_replay(server_plain, lat)

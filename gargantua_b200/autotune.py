@@ -4,7 +4,8 @@ chosen by timing candidates on the caller's own data.
 * Splat: gg_splat_autotune times gg_splat_bin under every brick edge and
   chunk (and direct atomics) on the given particles and keeps the fastest in
   the volume, per deposit mode.
-* Server: each candidate (chunk_rays, wave_rays, max_waves_in_flight) serves
+* Server: each candidate (schedule, chunk_rays, wave_rays,
+  max_waves_in_flight, refill cadence) serves
   the same sample of requests closed-loop on a fresh server; the candidate
   with the smallest device span (first launch to last, CUDA events) wins.
   The sample should look like the traffic to come: sizes, step budgets and
@@ -24,6 +25,7 @@ CHUNKS = (32, 64, 128)
 WAVES = (2 << 20, 4 << 20, 8 << 20)
 IN_FLIGHT = (2, 3)
 CADENCES = ((8, 8), (4, 4), (16, 8), (8, 16))  # (steps_per_round, refill_idle)
+SCHEDULES = (T.SCHEDULE_CHUNKS, T.SCHEDULE_LANE_REFILL)
 
 
 @dataclass
@@ -33,6 +35,7 @@ class ServerShape:
     max_waves_in_flight: int
     steps_per_round: int
     refill_idle: int
+    schedule: int
     span_seconds: float
     ray_steps: int
 
@@ -43,7 +46,7 @@ class ServerShape:
     def config(self) -> dict:
         return {"chunk_rays": self.chunk_rays, "wave_rays": self.wave_rays,
                 "max_waves_in_flight": self.max_waves_in_flight, "steps_per_round": self.steps_per_round,
-                "refill_idle": self.refill_idle}
+                "refill_idle": self.refill_idle, "schedule": self.schedule}
 
 
 def tune_splat(ps: H.Particles, vol: H.Volume) -> dict:
@@ -64,20 +67,22 @@ def _serve(ctx: H.Context, vol, specs, shape: dict, memory_bytes: int) -> Server
         steps = sum(int(server.wait(t)[2].ray_steps) for t in tickets)
         tot = server.totals(reset=True)
         return ServerShape(shape["chunk_rays"], shape["wave_rays"], shape["max_waves_in_flight"],
-                           shape["steps_per_round"], shape["refill_idle"], tot["span_seconds"], steps)
+                           shape["steps_per_round"], shape["refill_idle"], shape["schedule"], tot["span_seconds"],
+                           steps)
     finally:
         server.close()
 
 
 def tune_server(ctx: H.Context, vol, specs: list[H.RequestSpec], memory_bytes: int = 0, chunks=CHUNKS, waves=WAVES,
-                in_flight=IN_FLIGHT, cadences=CADENCES, repeats: int = 2) -> dict:
+                in_flight=IN_FLIGHT, cadences=CADENCES, schedules=SCHEDULES, repeats: int = 2) -> dict:
     """The fastest server shape for `specs`, found one group of settings at
-    a time (chunk and waves in flight, then wave size, then the refill
-    cadence), as ServerConfig keyword arguments, plus every trial's rate."""
+    a time (the schedule, chunk size and waves in flight, then wave size,
+    then, for the lane-refill schedule, its cadence), as ServerConfig
+    keyword arguments, plus every trial's rate."""
     if not specs:
         raise ValueError("tune_server needs a sample of requests")
     best = {"chunk_rays": chunks[0], "wave_rays": waves[len(waves) // 2], "max_waves_in_flight": in_flight[0],
-            "steps_per_round": cadences[0][0], "refill_idle": cadences[0][1]}
+            "steps_per_round": cadences[0][0], "refill_idle": cadences[0][1], "schedule": schedules[0]}
     _serve(ctx, vol, specs[:2], best, memory_bytes)  # build kernels, graphs, pools
     trials = []
 
@@ -87,11 +92,17 @@ def tune_server(ctx: H.Context, vol, specs: list[H.RequestSpec], memory_bytes: i
         return r
 
     groups = [
+        [{"schedule": sch} for sch in schedules],
         [{"chunk_rays": c, "max_waves_in_flight": f} for c in chunks for f in in_flight],
         [{"wave_rays": w} for w in waves],
         [{"steps_per_round": spr, "refill_idle": idle} for spr, idle in cadences],
     ]
     for group in groups:
+        if "steps_per_round" in group[0] and best["schedule"] != T.SCHEDULE_LANE_REFILL:
+            continue  # the cadence only matters to the lane-refill schedule
+        if len(group) == 1:
+            best = dict(best, **group[0])
+            continue
         results = []
         for change in group:
             shape = dict(best, **change)

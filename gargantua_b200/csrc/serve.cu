@@ -230,13 +230,77 @@ __device__ void serve_queue(const WaveArgs& a, uint32_t lane) {
     }
 }
 
-// One persistent kernel per metric; a wave runs both side by side.
+// The chunk schedule (GG_SCHEDULE_CHUNKS): a warp steals a chunk, gives
+// each lane one of its rays (32 at a time) and runs every lane to the end of
+// its ray with no warp-level operation inside the step loop, like a
+// thread-per-pixel image kernel; one warp-aggregated account per 32 rays.
+// The request's uniforms are copied to registers once per chunk, so the
+// step loop reads them as it would read kernel parameters.
+template <int Kind>
+__device__ void serve_chunks(const WaveArgs& a, uint32_t lane) {
+    const ServeChunk* chunks = Kind == 0 ? a.chunks0 : a.chunks1;
+    const uint32_t nchunks = a.header->chunk_count[Kind];
+    uint32_t* head = &a.header->heads[Kind];
+    for (uint32_t round = 0; round < kMaxRounds; ++round) {
+        uint32_t c = 0;
+        if (lane == 0) c = atomicAdd(head, 1u);
+        c = __shfl_sync(kFull, c, 0);
+        if (c >= nchunks) break;
+        const ServeChunk ch = chunks[c];
+        const ServeRequest& R = a.requests[ch.request];
+        const MarchUniforms u = R.u;
+        const cudaTextureObject_t em = R.emission, vel = R.velocity;
+        for (uint32_t base = 0; base < ch.count; base += 32u) {
+            const uint32_t k = base + lane;
+            const bool has = k < ch.count;
+            PixelResult r{};
+            if (has) {
+                const uint32_t pixel = ch.first + k;
+                const uint32_t w = u.resolution.x;
+                float3 dir = camera_direction(u, pixel % w, pixel / w);
+                float3 origin = to_f3(u.cameraPosition);
+                typename LaneOf<Kind>::type L;
+                if constexpr (Kind == 0) {
+                    float3 sky;
+                    SweepTables t{a.sphere_table, R.camera_table, R.sky_table};
+                    if (s_init(L, origin, dir, u, t, &sky)) {
+                        r = sky_only_result(sky, u, a.blackbody);
+                        write_result(R, pixel, r);
+                    } else {
+                        for (uint32_t s = 0; s <= STEP_CAP_STILL; ++s)
+                            if (s_step(L, u, em, vel, em != 0)) break;
+                        r = s_finish(L, u, t, a.blackbody);
+                        complete(a, ch.request, pixel, r);
+                    }
+                } else {
+                    k_init(L, origin, dir, u);
+                    for (uint32_t s = 0; s <= STEP_CAP_STILL; ++s)
+                        if (k_step(L, u, em, vel, em != 0)) break;
+                    r = k_finish(L, u, a.blackbody);
+                    complete(a, ch.request, pixel, r);
+                }
+            }
+            account(a, has, ch.request, r, u.driftBudget, lane);
+        }
+    }
+}
+
+// One persistent kernel per metric and schedule; a wave runs the two
+// metrics side by side.
 __global__ void __launch_bounds__(kServeThreads) serve_schwarzschild_kernel(WaveArgs a) {
     serve_queue<0>(a, threadIdx.x & 31u);
 }
 
 __global__ void __launch_bounds__(kServeThreads) serve_kerr_kernel(WaveArgs a) {
     serve_queue<1>(a, threadIdx.x & 31u);
+}
+
+__global__ void __launch_bounds__(kServeThreads) serve_schwarzschild_chunks_kernel(WaveArgs a) {
+    serve_chunks<0>(a, threadIdx.x & 31u);
+}
+
+__global__ void __launch_bounds__(kServeThreads) serve_kerr_chunks_kernel(WaveArgs a) {
+    serve_chunks<1>(a, threadIdx.x & 31u);
 }
 
 // FP64 re-integration of the wave's flagged rays.
@@ -394,8 +458,13 @@ static int capture_wave_graph(gg_server* s, WaveSlot& w) {
     GG_CUDA(cudaStreamBeginCapture(w.stream, cudaStreamCaptureModeThreadLocal), "wave capture");
     GG_CUDA(cudaEventRecord(w.fork, w.stream), "wave capture");
     GG_CUDA(cudaStreamWaitEvent(w.side, w.fork, 0), "wave capture");
-    serve_schwarzschild_kernel<<<s->grid_s, kServeThreads, 0, w.side>>>(w.args);
-    serve_kerr_kernel<<<s->grid_k, kServeThreads, 0, w.stream>>>(w.args);
+    if (s->cfg.schedule == GG_SCHEDULE_LANE_REFILL) {
+        serve_schwarzschild_kernel<<<s->grid_s, kServeThreads, 0, w.side>>>(w.args);
+        serve_kerr_kernel<<<s->grid_k, kServeThreads, 0, w.stream>>>(w.args);
+    } else {
+        serve_schwarzschild_chunks_kernel<<<s->grid_s, kServeThreads, 0, w.side>>>(w.args);
+        serve_kerr_chunks_kernel<<<s->grid_k, kServeThreads, 0, w.stream>>>(w.args);
+    }
     GG_CUDA(cudaEventRecord(w.join, w.side), "wave capture");
     GG_CUDA(cudaStreamWaitEvent(w.stream, w.join, 0), "wave capture");
     cudaError_t e = cudaStreamEndCapture(w.stream, &g);
@@ -721,6 +790,8 @@ GG_API int gg_server_create(gg_context* ctx, const gg_volume* vol, const gg_serv
                         s->cfg.steps_per_round, s->cfg.refill_idle);
     if (s->cfg.fp64_policy != GG_FP64_ESCAPING && s->cfg.fp64_policy != GG_FP64_ALL_FLAGGED)
         return gg::fail(GG_ERR_INVALID_ARGUMENT, "Unknown FP64 policy %u.", s->cfg.fp64_policy);
+    if (s->cfg.schedule != GG_SCHEDULE_CHUNKS && s->cfg.schedule != GG_SCHEDULE_LANE_REFILL)
+        return gg::fail(GG_ERR_INVALID_ARGUMENT, "Unknown schedule %u.", s->cfg.schedule);
     if (s->cfg.memory_bytes == 0) s->cfg.memory_bytes = (ctx->budget - ctx->used) / 4;
     if (ctx->used + s->cfg.memory_bytes > ctx->budget)
         return gg::fail(GG_ERR_OVER_BUDGET, "The server asks for %llu bytes but the budget has %llu left.",
@@ -735,10 +806,16 @@ GG_API int gg_server_create(gg_context* ctx, const gg_volume* vol, const gg_serv
     s->flagged_capacity = s->cfg.wave_rays / 8;
     s->slot_bytes = gg::slot_offset_flagged(s.get()) + (uint64_t)s->flagged_capacity * 8u;
     int blocks = 0;
-    GG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, gg::serve_schwarzschild_kernel, gg::kServeThreads, 0),
+    const bool refill = s->cfg.schedule == GG_SCHEDULE_LANE_REFILL;
+    GG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                &blocks, refill ? (const void*)gg::serve_schwarzschild_kernel : (const void*)gg::serve_schwarzschild_chunks_kernel,
+                gg::kServeThreads, 0),
             "occupancy");
     s->grid_s = std::max(1, blocks) * ctx->sm_count;
-    GG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&blocks, gg::serve_kerr_kernel, gg::kServeThreads, 0), "occupancy");
+    GG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(
+                &blocks, refill ? (const void*)gg::serve_kerr_kernel : (const void*)gg::serve_kerr_chunks_kernel,
+                gg::kServeThreads, 0),
+            "occupancy");
     s->grid_k = std::max(1, blocks) * ctx->sm_count;
     GG_CUDA(cudaStreamCreateWithFlags(&s->build, cudaStreamNonBlocking), "server streams");
     GG_CUDA(cudaStreamCreateWithFlags(&s->copy, cudaStreamNonBlocking), "server streams");

@@ -608,11 +608,12 @@ class Server:
 
     def __init__(self, ctx: Context, vol: Volume | None, mode: int = T.SERVE_BATCHED, memory_bytes: int = 0,
                  wave_rays: int = 0, chunk_rays: int = 0, max_waves_in_flight: int = 0,
-                 fp64_policy: int = T.FP64_ESCAPING, steps_per_round: int = 0, refill_idle: int = 0):
+                 fp64_policy: int = T.FP64_ESCAPING, steps_per_round: int = 0, refill_idle: int = 0,
+                 schedule: int = T.SCHEDULE_CHUNKS):
         self.ctx = ctx
         self.handle = C.c_void_p()
         cfg = T.ServerConfig(mode, memory_bytes, wave_rays, chunk_rays, max_waves_in_flight, fp64_policy,
-                             steps_per_round, refill_idle)
+                             steps_per_round, refill_idle, schedule)
         check(lib().gg_server_create(ctx.handle, vol.handle if vol else None, C.byref(cfg), C.byref(self.handle)))
         ctx.adopt(self)
         self._buffers = {}

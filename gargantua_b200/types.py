@@ -153,7 +153,11 @@ class RequestResult(C.Structure):
 
 class ServerConfig(C.Structure):
     _fields_ = [("mode", C.c_int), ("memory_bytes", C.c_uint64), ("wave_rays", u32), ("chunk_rays", u32),
-                ("max_waves_in_flight", u32), ("fp64_policy", u32), ("steps_per_round", u32), ("refill_idle", u32)]
+                ("max_waves_in_flight", u32), ("fp64_policy", u32), ("steps_per_round", u32), ("refill_idle", u32),
+                ("schedule", u32)]
+
+
+SCHEDULE_CHUNKS, SCHEDULE_LANE_REFILL = 0, 1
 
 
 FP64_ESCAPING, FP64_ALL_FLAGGED = 0, 1

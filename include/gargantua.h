@@ -427,6 +427,18 @@ typedef enum {
     GG_SERVE_SERIAL_PLAIN_AS_WRITTEN = 2
 } gg_serve_mode;
 
+/* How the persistent serve kernels hand rays to lanes. Both steal chunks of
+ * rays with one atomic per warp and give the same pixels. */
+typedef enum {
+    /* A warp takes a chunk, runs each lane's ray to its end, then takes the
+     * next: no warp-level work inside the step loop (the default, faster
+     * on B200 on the served mix). */
+    GG_SCHEDULE_CHUNKS = 0,
+    /* Lanes that finish are refilled with new rays between rounds of
+     * steps_per_round steps once refill_idle lanes are idle. */
+    GG_SCHEDULE_LANE_REFILL = 1
+} gg_schedule;
+
 typedef struct {
     int mode;                  /* gg_serve_mode */
     uint64_t memory_bytes;     /* device memory for admitted requests' targets; 0: a quarter of the budget left */
@@ -434,8 +446,9 @@ typedef struct {
     uint32_t chunk_rays;       /* rays per work-stealing chunk; 0: 32, one per lane of a warp */
     uint32_t max_waves_in_flight; /* 0: 2 */
     uint32_t fp64_policy;      /* gg_fp64_policy */
-    uint32_t steps_per_round;  /* RK4 steps a warp takes between refills of idle lanes; 0: 8 */
-    uint32_t refill_idle;      /* idle lanes of a warp that trigger a refill; 0: 8 */
+    uint32_t steps_per_round;  /* lane refill: RK4 steps a warp takes between refills of idle lanes; 0: 8 */
+    uint32_t refill_idle;      /* lane refill: idle lanes of a warp that trigger a refill; 0: 8 */
+    uint32_t schedule;         /* gg_schedule */
 } gg_server_config;
 
 /* A server over a resident volume (vol may be NULL: no gas). */

@@ -122,7 +122,7 @@ def test_library_structs_match_their_ctypes_mirrors(tmp_path):
         "gg_request": (T.Request, ["azimuth", "width", "flags", "output", "debug_output", "volume"]),
         "gg_request_result": (T.RequestResult, ["submitted", "ray_steps", "counters", "status"]),
         "gg_server_config": (T.ServerConfig, ["mode", "memory_bytes", "wave_rays", "max_waves_in_flight",
-                                             "fp64_policy", "steps_per_round", "refill_idle"]),
+                                             "fp64_policy", "steps_per_round", "refill_idle", "schedule"]),
     }
     lines = ['#include <stdio.h>', '#include <stddef.h>', '#include "gargantua.h"', "int main(void){"]
     for cname, (_, fields) in checks.items():

@@ -146,11 +146,13 @@ def test_server_autotune_picks_a_measured_candidate(world):
 
     specs = mix_specs()[:4]
     tuned = autotune.tune_server(world["ctx"], world["vol"], specs, chunks=(32, 64), waves=(1 << 20,),
-                                 in_flight=(2,), cadences=((8, 8), (4, 4)), repeats=1)
+                                 in_flight=(2,), cadences=((8, 8), (4, 4)),
+                                 schedules=(g.types.SCHEDULE_LANE_REFILL,), repeats=1)
     assert tuned["chunk_rays"] in (32, 64) and tuned["rate"] > 0.0
     assert (tuned["steps_per_round"], tuned["refill_idle"]) in ((8, 8), (4, 4))
-    assert len(tuned["trials"]) == 5
-    shape = {k: tuned[k] for k in ("chunk_rays", "wave_rays", "max_waves_in_flight", "steps_per_round", "refill_idle")}
+    assert len(tuned["trials"]) == 4  # two chunk sizes, then two cadences
+    shape = {k: tuned[k] for k in ("chunk_rays", "wave_rays", "max_waves_in_flight", "steps_per_round", "refill_idle",
+                                   "schedule")}
     server = g.Server(world["ctx"], world["vol"], g.types.SERVE_BATCHED, **shape)
     pixels, _, res = server.wait(server.submit(specs[0]))
     assert res.status == 0 and res.counters.rays == specs[0].width * specs[0].height
@@ -211,3 +213,19 @@ def test_fp64_policy_skips_captured_rays_by_default(world):
     assert counts[g.types.FP64_ALL_FLAGGED] > counts[g.types.FP64_ESCAPING]
     a, b = lum[g.types.FP64_ESCAPING], lum[g.types.FP64_ALL_FLAGGED]
     assert np.abs(a - b).sum() / max(b.sum(), 1e-30) < 1e-3
+
+
+def test_schedules_give_the_same_pixels(world):
+    """The chunk and lane-refill schedules march the same rays with the same
+    arithmetic: identical pixels for every request of a mix."""
+    import gargantua_b200 as g
+
+    specs = mix_specs()
+    out = {}
+    for sch in (g.types.SCHEDULE_CHUNKS, g.types.SCHEDULE_LANE_REFILL):
+        server = g.Server(world["ctx"], world["vol"], g.types.SERVE_BATCHED, schedule=sch)
+        out[sch] = run(server, specs)
+        server.close()
+    for (pa, _, ra), (pb, _, rb) in zip(out[g.types.SCHEDULE_CHUNKS], out[g.types.SCHEDULE_LANE_REFILL]):
+        assert np.array_equal(pa.view(np.uint16), pb.view(np.uint16))
+        assert ra.ray_steps == rb.ray_steps and ra.counters.rays == rb.counters.rays
