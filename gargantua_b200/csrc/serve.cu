@@ -424,6 +424,10 @@ struct gg_server {
     uint64_t slot_bytes = 0;
     int grid_s = 0, grid_k = 0;
     cudaStream_t build = nullptr, copy = nullptr, plain = nullptr;
+    // The server's own stream-ordered pool, keeping up to memory_bytes mapped
+    // between requests so freeing one request's targets and allocating the
+    // next costs no page mapping at synchronisation points.
+    cudaMemPool_t pool = nullptr;
     cudaEvent_t built = nullptr, origin = nullptr;
     std::vector<gg::WaveSlot> slots;
     std::mutex mu;
@@ -486,13 +490,16 @@ static bool serial(const gg_server* s) { return s->cfg.mode != GG_SERVE_BATCHED;
 static int admit(gg_server* s, const std::shared_ptr<ServedRequest>& r) {
     gg_context* ctx = s->ctx;
     const uint64_t px = r->rays;
-    GG_CUDA(cudaMallocAsync((void**)&r->d_color, px * 8u, s->build), "request target");
-    if (r->q.debug_output) GG_CUDA(cudaMallocAsync((void**)&r->d_debug, px * 8u, s->build), "request debug target");
-    GG_CUDA(cudaMallocAsync((void**)&r->d_stats, 128, s->build), "request counters");
+    GG_CUDA(cudaMallocFromPoolAsync((void**)&r->d_color, px * 8u, s->pool, s->build), "request target");
+    if (r->q.debug_output)
+        GG_CUDA(cudaMallocFromPoolAsync((void**)&r->d_debug, px * 8u, s->pool, s->build), "request debug target");
+    GG_CUDA(cudaMallocFromPoolAsync((void**)&r->d_stats, 128, s->pool, s->build), "request counters");
     GG_CUDA(cudaMemsetAsync(r->d_stats, 0, 128, s->build), "request counters");
     if (r->q.spin == 0.0f) {
-        GG_CUDA(cudaMallocAsync((void**)&r->sweep.camera, SWEEP_TABLE_SIZE * sizeof(float), s->build), "camera table");
-        GG_CUDA(cudaMallocAsync((void**)&r->sweep.sky, SWEEP_TABLE_SIZE * sizeof(float), s->build), "sky table");
+        GG_CUDA(cudaMallocFromPoolAsync((void**)&r->sweep.camera, SWEEP_TABLE_SIZE * sizeof(float), s->pool, s->build),
+                "camera table");
+        GG_CUDA(cudaMallocFromPoolAsync((void**)&r->sweep.sky, SWEEP_TABLE_SIZE * sizeof(float), s->pool, s->build),
+                "sky table");
         GG_CHECK(sweep_build(ctx, s->build, (double)r->q.distance, &r->sweep));
         sweep_apply(ctx, &r->sweep, &r->u);
     }
@@ -817,6 +824,15 @@ GG_API int gg_server_create(gg_context* ctx, const gg_volume* vol, const gg_serv
                 gg::kServeThreads, 0),
             "occupancy");
     s->grid_k = std::max(1, blocks) * ctx->sm_count;
+    {
+        cudaMemPoolProps props{};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = ctx->device;
+        GG_CUDA(cudaMemPoolCreate(&s->pool, &props), "server memory pool");
+        uint64_t keep = s->cfg.memory_bytes;
+        GG_CUDA(cudaMemPoolSetAttribute(s->pool, cudaMemPoolAttrReleaseThreshold, &keep), "server memory pool");
+    }
     GG_CUDA(cudaStreamCreateWithFlags(&s->build, cudaStreamNonBlocking), "server streams");
     GG_CUDA(cudaStreamCreateWithFlags(&s->copy, cudaStreamNonBlocking), "server streams");
     GG_CUDA(cudaStreamCreateWithFlags(&s->plain, cudaStreamNonBlocking), "server streams");
@@ -893,6 +909,7 @@ GG_API void gg_server_destroy(gg_server* s) {
     cudaStreamDestroy(s->build);
     cudaStreamDestroy(s->copy);
     cudaStreamDestroy(s->plain);
+    if (s->pool) cudaMemPoolDestroy(s->pool);
     delete s;
 }
 
