@@ -292,20 +292,40 @@ __global__ void __launch_bounds__(kBrickBlock) brick_deposit_kernel(BrickArgs a)
     const int ox = (int)(bx * B), oy = (int)(by * B), oz = (int)(bz * B);
     for (uint32_t w = threadIdx.x; w < kWords; w += blockDim.x) tile[w] = 0u;
     __syncthreads();
-    for (uint32_t k = begin + threadIdx.x; k < end; k += blockDim.x) {
-        const uint32_t i = a.sorted[k];
-        Footprint f;
-        // Always inside and in this brick (the count pass put it here); the
-        // test keeps every tile index in bounds regardless.
-        if (!footprint(a.pos[i], a.u, f)) continue;
-        if ((uint32_t)(f.lx - ox) >= B || (uint32_t)(f.ly - oy) >= B || (uint32_t)(f.lz - oz) >= B) continue;
-        const float4 v = a.vel[i];
-        for_each_corner(f, a.u, a.first_index + i, [&](int x, int y, int z, float w) {
-            Deposit d = deposit_values(w, f.energy, f.relative, v.x, v.y, v.z);
-            uint32_t* rec = tile + 6u * (((uint32_t)(z - oz) * T + (uint32_t)(y - oy)) * T + (uint32_t)(x - ox));
+    // kGather particles per thread per pass: their slots, then their
+    // positions and velocities, are loaded before any is deposited, so the
+    // random gathers overlap instead of following one another.
+    constexpr uint32_t kGather = 4;
+    for (uint32_t k0 = begin + threadIdx.x; k0 < end; k0 += kGather * blockDim.x) {
+        uint32_t idx[kGather];
+        float4 pos[kGather], vel[kGather];
 #pragma unroll
-            for (int c = 0; c < 6; ++c) atomicAdd(rec + c, d.w[c]);
-        });
+        for (uint32_t j = 0; j < kGather; ++j) {
+            const uint32_t k = k0 + j * blockDim.x;
+            idx[j] = k < end ? a.sorted[k] : kOutside;
+        }
+#pragma unroll
+        for (uint32_t j = 0; j < kGather; ++j) {
+            if (idx[j] == kOutside) continue;
+            pos[j] = a.pos[idx[j]];
+            vel[j] = a.vel[idx[j]];
+        }
+#pragma unroll
+        for (uint32_t j = 0; j < kGather; ++j) {
+            if (idx[j] == kOutside) continue;
+            Footprint f;
+            // Always inside and in this brick (the count pass put it here);
+            // the test keeps every tile index in bounds regardless.
+            if (!footprint(pos[j], a.u, f)) continue;
+            if ((uint32_t)(f.lx - ox) >= B || (uint32_t)(f.ly - oy) >= B || (uint32_t)(f.lz - oz) >= B) continue;
+            const float4 v = vel[j];
+            for_each_corner(f, a.u, a.first_index + idx[j], [&](int x, int y, int z, float w) {
+                Deposit d = deposit_values(w, f.energy, f.relative, v.x, v.y, v.z);
+                uint32_t* rec = tile + 6u * (((uint32_t)(z - oz) * T + (uint32_t)(y - oy)) * T + (uint32_t)(x - ox));
+#pragma unroll
+                for (int c = 0; c < 6; ++c) atomicAdd(rec + c, d.w[c]);
+            });
+        }
     }
     __syncthreads();
     const uint32_t n = a.u.volumeSize;
