@@ -83,6 +83,7 @@ SIGNATURES = {
     "gg_volume_write": (i, [vp, vp, vp]),
     "gg_tables_update": (i, [vp, C.c_float, P(T.MarchUniforms)]),
     "gg_tables_read": (i, [vp, vp, vp, vp]),
+    "gg_context_set_march_block": (i, [vp, u32, u32]),
     "gg_context_set_fp64_policy": (i, [vp, i]),
     "gg_targets_create": (i, [vp, u32, u32, P(vp)]),
     "gg_targets_destroy": (None, [vp]),

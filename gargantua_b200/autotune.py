@@ -4,6 +4,8 @@ chosen by timing candidates on the caller's own data.
 * Splat: gg_splat_autotune times gg_splat_bin under every brick edge and
   chunk (and direct atomics) on the given particles and keeps the fastest in
   the volume, per deposit mode.
+* March: the image kernels' thread block, timed on a frame of the caller's
+  shape (tune_march_block).
 * Server: each candidate (schedule, chunk_rays, wave_rays,
   max_waves_in_flight, refill cadence) serves
   the same sample of requests closed-loop on a fresh server; the candidate
@@ -110,3 +112,38 @@ def tune_server(ctx: H.Context, vol, specs: list[H.RequestSpec], memory_bytes: i
         best = max(results, key=lambda t: t.rate).config()
     win = max((t for t in trials if t.config() == best), key=lambda t: t.rate)
     return dict(best, rate=win.rate, trials=[dict(t.config(), rate=t.rate) for t in trials])
+
+
+MARCH_BLOCKS = ((8, 8), (16, 4), (32, 2), (8, 4), (16, 8), (32, 4), (8, 16), (16, 16), (32, 8))
+
+
+def tune_march_block(ctx: H.Context, vol, u: T.MarchUniforms, precision: int = T.PRECISION_PLAIN,
+                     blocks=MARCH_BLOCKS, repeats: int = 3) -> dict:
+    """The image kernels' thread block for this frame shape: gg_march timed
+    (CUDA events on the context's stream) under each block shape; the
+    context keeps the fastest."""
+    import torch
+
+    w, h = u.resolution.x, u.resolution.y
+    ext = torch.cuda.ExternalStream(H.lib().gg_context_stream(ctx.handle))
+    targets = H.Targets(ctx, w, h)
+    times = {}
+    try:
+        for bw, bh in blocks:
+            ctx.set_march_block(bw, bh)
+            H.march(ctx, vol, u, targets, precision)  # warm
+            best = float("inf")
+            for _ in range(repeats):
+                e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+                e0.record(ext)
+                H.march(ctx, vol, u, targets, precision)
+                e1.record(ext)
+                ext.synchronize()
+                best = min(best, e0.elapsed_time(e1))
+            times[(bw, bh)] = best
+    finally:
+        targets.close()
+    win = min(times, key=times.get)
+    ctx.set_march_block(*win)
+    return {"block": list(win), "ms": times[win], "trials": [{"block": list(k), "ms": v} for k, v in times.items()]}
+

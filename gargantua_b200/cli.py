@@ -288,6 +288,10 @@ def bench(o: Options) -> dict:
         if o.spin == 0.0:
             ctx.enable_tables(ub, float(cam.distance))
         report["bake_full"] = _timing(lambda: bake.bake_full(ub), sync, iterations=5)
+        bake.overflow(reset=True)
+        bake.bake_full(ub)
+        sync()
+        report["bake_truncated_rays"] = bake.overflow()  # rays whose samples overran BAKE_SAMPLES
         report["walk"] = _timing(lambda: bake.walk(vol, ub, targets), sync)
         bake.close()
     targets.close()

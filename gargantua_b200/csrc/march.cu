@@ -14,7 +14,7 @@ namespace gg {
 
 // Mode: GG_PRECISION_PLAIN, _COMPENSATED or _PLAIN_AS_WRITTEN.
 template <int Mode>
-__global__ void __launch_bounds__(64) march_image_kernel(MarchParams p) {
+__global__ void __launch_bounds__(256) march_image_kernel(MarchParams p) {
     constexpr bool Comp = Mode == GG_PRECISION_COMPENSATED;
     const uint32_t gx = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t gy = blockIdx.y * blockDim.y + threadIdx.y;
@@ -212,6 +212,8 @@ MarchParams make_params(gg_context* ctx, const gg_volume* vol, const MarchUnifor
     p.velocity = vol ? vol->velocity_tex : 0;
     p.blackbody = ctx->blackbody;
     p.fp64_all = ctx->fp64_policy == GG_FP64_ALL_FLAGGED ? 1u : 0u;
+    p.block_w = ctx->march_block_w;
+    p.block_h = ctx->march_block_h;
     return p;
 }
 
@@ -219,7 +221,7 @@ MarchParams make_params(gg_context* ctx, const gg_volume* vol, const MarchUnifor
 // whose flagged list and counter are already set (p.flagged, p.flagged_count
 // zeroed by the caller, p.flagged_capacity entries).
 int launch_compensated_image(const MarchParams& p, cudaStream_t stream, int sm_count) {
-    dim3 block(MARCH_THREADGROUP_WIDTH, MARCH_THREADGROUP_HEIGHT);
+    dim3 block(p.block_w, p.block_h);
     dim3 grid((p.target_width + block.x - 1) / block.x, (p.target_height + block.y - 1) / block.y);
     march_image_kernel<GG_PRECISION_COMPENSATED><<<grid, block, 0, stream>>>(p);
     GG_CHECK(launch_status("compensated march"));
@@ -228,7 +230,7 @@ int launch_compensated_image(const MarchParams& p, cudaStream_t stream, int sm_c
 }
 
 int launch_plain_image(const MarchParams& p, cudaStream_t stream, bool as_written) {
-    dim3 block(MARCH_THREADGROUP_WIDTH, MARCH_THREADGROUP_HEIGHT);
+    dim3 block(p.block_w, p.block_h);
     dim3 grid((p.target_width + block.x - 1) / block.x, (p.target_height + block.y - 1) / block.y);
     if (as_written) march_image_kernel<GG_PRECISION_PLAIN_AS_WRITTEN><<<grid, block, 0, stream>>>(p);
     else march_image_kernel<GG_PRECISION_PLAIN><<<grid, block, 0, stream>>>(p);
@@ -318,6 +320,18 @@ GG_API int gg_targets_read(gg_targets* t, uint16_t* color, uint16_t* debug, floa
     return GG_OK;
 }
 
+GG_API int gg_context_set_march_block(gg_context* ctx, uint32_t width, uint32_t height) {
+    const uint32_t threads = width * height;
+    if (!ctx || width == 0 || height == 0 || width > 256 || height > 256 || threads < 32 || threads > 256 ||
+        threads % 32u != 0)
+        return gg::fail(GG_ERR_INVALID_ARGUMENT, "March block %ux%u is not 32..256 threads in whole warps.", width,
+                        height);
+    std::lock_guard<std::recursive_mutex> lock(ctx->mu);
+    ctx->march_block_w = width;
+    ctx->march_block_h = height;
+    return GG_OK;
+}
+
 GG_API int gg_context_set_fp64_policy(gg_context* ctx, int policy) {
     if (!ctx || (policy != GG_FP64_ESCAPING && policy != GG_FP64_ALL_FLAGGED))
         return gg::fail(GG_ERR_INVALID_ARGUMENT, "gg_context_set_fp64_policy needs a context and a known policy.");
@@ -370,7 +384,7 @@ GG_API int gg_march(gg_context* ctx, const gg_volume* vol, const MarchUniforms* 
         p.flagged_capacity = (uint32_t)entries;
         GG_CUDA(cudaMemsetAsync(ctx->flagged, 0, 4u, ctx->stream), "re-integration list reset");
     }
-    dim3 block(MARCH_THREADGROUP_WIDTH, MARCH_THREADGROUP_HEIGHT);
+    dim3 block(p.block_w, p.block_h);
     dim3 grid((targets->width + block.x - 1) / block.x, (targets->height + block.y - 1) / block.y);
     if (comp) {
         march_image_kernel<GG_PRECISION_COMPENSATED><<<grid, block, 0, ctx->stream>>>(p);

@@ -30,6 +30,7 @@ struct MarchParams {
     uint32_t* flagged_count;  // its length, a device counter
     uint32_t flagged_capacity;
     uint32_t fp64_all;        // GG_FP64_ALL_FLAGGED: captured rays are re-integrated too
+    uint32_t block_w, block_h;  // image kernel block shape
 };
 
 struct MarchResult {

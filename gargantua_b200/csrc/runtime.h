@@ -74,6 +74,8 @@ struct gg_context {
     MarchCounters* counters = nullptr;
     unsigned long long* stats = nullptr;  // last march: ray steps, samples, FP64 rays, spare
     int fp64_policy = 0;  // gg_fp64_policy of gg_march and gg_probe
+    uint32_t march_block_w = MARCH_THREADGROUP_WIDTH;   // image kernel block (gg_context_set_march_block)
+    uint32_t march_block_h = MARCH_THREADGROUP_HEIGHT;
     void* probe_buffer = nullptr;
     uint64_t probe_capacity = 0;  // bytes
     uint32_t* flagged = nullptr;  // FP64 re-integration list

@@ -260,6 +260,10 @@ class Context:
                                         C.byref(t)))
         return t.value
 
+    def set_march_block(self, width: int, height: int):
+        """gg_context_set_march_block: the image kernels' thread block."""
+        check(lib().gg_context_set_march_block(self.handle, width, height))
+
     def set_fp64_policy(self, policy: int):
         """gg_context_set_fp64_policy for gg_march and gg_probe."""
         check(lib().gg_context_set_fp64_policy(self.handle, policy))
