@@ -4,7 +4,7 @@
  * walk, tone curve) as sm_100a kernels behind a plain C interface.
  *
  * The interface replaces the Metal passes a gargantua host encodes
- * (Sources/Gargantua/Passes/*.swift) one for one. Structs are the
+ * (the Swift files of Sources/Gargantua/Passes) one for one. Structs are the
  * ShaderTypes.h layouts (gargantua_types.h). Every handle is opaque and owned
  * by the library; device state (particles, volumes, tables, targets) stays
  * resident between calls. Host pointers passed in are caller-owned and are
@@ -272,6 +272,12 @@ typedef enum {
     /* Every flagged ray, captured ones included. */
     GG_FP64_ALL_FLAGGED = 1
 } gg_fp64_policy;
+
+/* Thread block of the image kernels (gg_march, gg_march_compensated_noalloc
+ * and the serial serving modes) on this context: width x height pixels,
+ * 32..256 threads in whole warps. Default 8x8, the reference's threadgroup
+ * (MarchPass.swift:101). */
+GG_API int gg_context_set_march_block(gg_context* ctx, uint32_t width, uint32_t height);
 
 /* The policy gg_march and gg_probe use on this context. */
 GG_API int gg_context_set_fp64_policy(gg_context* ctx, int policy);
