@@ -135,8 +135,8 @@ struct gg_volume {
     uint64_t bytes = 0;
     // Splat shape per deposit mode ([0] stochastic, [1] exact): brick edge B
     // (0: direct global atomics) and particles per deposit work item.
-    uint32_t brick_edge[2] = {8u, 8u};
-    uint32_t brick_chunk[2] = {4096u, 2048u};
+    uint32_t brick_edge[2] = {0u, 8u};    // [stochastic, exact]; set per size by gg_volume_create
+    uint32_t brick_chunk[2] = {0u, 1024u};
     void* brick_scratch = nullptr;  // counts, offsets, cursor, items, sorted slots, keys
     uint64_t brick_scratch_capacity = 0;
 };

@@ -277,8 +277,13 @@ __device__ __forceinline__ uint32_t item_brick(const uint32_t* items, uint32_t b
     return lo;
 }
 
+// Threads of a deposit block. A 16^3 brick's 17^3 six-word tile takes 118 KB of
+// shared memory, so one block fills an SM: it gets 1024 threads to keep enough
+// shared atomics in flight; the smaller tiles fit several 256-thread blocks.
+template <uint32_t B> constexpr uint32_t deposit_threads() { return B == 16u ? 1024u : kBrickBlock; }
+
 template <uint32_t B>
-__global__ void __launch_bounds__(kBrickBlock) brick_deposit_kernel(BrickArgs a) {
+__global__ void __launch_bounds__(deposit_threads<B>()) brick_deposit_kernel(BrickArgs a) {
     constexpr uint32_t T = B + 1;
     constexpr uint32_t kWords = T * T * T * 6u;
     extern __shared__ uint32_t tile[];
@@ -498,12 +503,12 @@ static int splat_bin_shaped(gg_particles* ps, gg_volume* vol, const SplatUniform
     // Work items number at most count / chunk + one per non-empty brick.
     const uint32_t grid = (ps->count + chunk - 1u) / chunk + bricks;
     if (edge == 4u) {
-        brick_deposit_kernel<4><<<grid, kBrickBlock, tile_bytes<4>(), ctx->stream>>>(a);
+        brick_deposit_kernel<4><<<grid, deposit_threads<4>(), tile_bytes<4>(), ctx->stream>>>(a);
     } else if (edge == 8u) {
-        brick_deposit_kernel<8><<<grid, kBrickBlock, tile_bytes<8>(), ctx->stream>>>(a);
+        brick_deposit_kernel<8><<<grid, deposit_threads<8>(), tile_bytes<8>(), ctx->stream>>>(a);
     } else {
         GG_CHECK(allow_shared((const void*)brick_deposit_kernel<16>, (int)tile_bytes<16>(), ctx->device, 2));
-        brick_deposit_kernel<16><<<grid, kBrickBlock, tile_bytes<16>(), ctx->stream>>>(a);
+        brick_deposit_kernel<16><<<grid, deposit_threads<16>(), tile_bytes<16>(), ctx->stream>>>(a);
     }
     return gg::launch_status("brick deposit");
 }
@@ -539,6 +544,16 @@ GG_API int gg_volume_create(gg_context* ctx, uint32_t size, gg_volume** out) {
     gg_volume* vol = new gg_volume();
     vol->ctx = ctx;
     vol->size = size;
+    // Default shapes, from timing every shape on the presets' settled disks
+    // (250k/96^3, 1M/128^3, 4M/256^3, uniform and concentrated): the
+    // stochastic deposit (one corner per particle) is fastest with direct
+    // global atomics at every size; the exact one with 8^3 bricks up to 128^3
+    // and with 16^3 bricks above, where 8^3 bricks make a histogram too large
+    // for more than one count block per SM.
+    vol->brick_edge[0] = 0u;
+    vol->brick_chunk[0] = 0u;
+    vol->brick_edge[1] = size > 128u ? 16u : 8u;
+    vol->brick_chunk[1] = size > 128u ? 16384u : 1024u;
     int s = gg::device_alloc(ctx, sums_bytes, (void**)&vol->sums, "volume sums");
     if (s == GG_OK) s = gg::cuda_status(cudaMemsetAsync(vol->sums, 0, sums_bytes, ctx->stream), "volume clear");
     cudaChannelFormatDesc desc = cudaCreateChannelDescHalf4();
