@@ -286,9 +286,8 @@ __device__ __forceinline__ bool s_step(SLane<R>& l, const MarchUniforms& u, cuda
     float3 pf = to_float3(position);
     if (gather && in_slab(pf, u.volumeHalfExtent) && l.transmittance > 0.004f) {
         float f = (float)fmaT(R(-2), rcp(l.s.r), R(1));
-        float3 dir = to_float3(s_direction(l, sn, cs));
-        gather_sample(gather_view(u, em, vel), pf, f, dir, path, l.travelled, l.color, l.transmittance,
-                      l.weighted_depth, l.depth_weight, l.samples);
+        gather_sample_with(gather_view(u, em, vel), pf, f, [&] { return to_float3(s_direction(l, sn, cs)); }, path,
+                           l.travelled, l.color, l.transmittance, l.weighted_depth, l.depth_weight, l.samples);
     }
     l.previous = position;
     if (u.sphereRadius > 0.0f && l.s.r >= sphere && l.s.rd > R(0)) {
@@ -454,10 +453,19 @@ template <typename R> __device__ __forceinline__ KState<R> k_offset(const KState
 // sin and cos of theta0 + delta from those of theta0, for |delta| <= 0.35:
 // the angle-addition formulas with Taylor polynomials of sin delta (through
 // delta^7, remainder below 2.2e-10) and cos delta (through delta^8,
-// remainder below 8e-12). False (nothing written) for larger |delta|.
+// remainder below 8e-12); for |delta| <= 0.02, the usual size of a stage's
+// offset, through delta^3 and delta^4 (remainders below 2.7e-11 and 9e-14).
+// False (nothing written) for larger |delta|.
 __device__ __forceinline__ bool sincos_shift(float st0, float ct0, float delta, float* st, float* ct) {
     if (!(fabsf(delta) <= 0.35f)) return false;
     float d2 = delta * delta;
+    if (fabsf(delta) <= 0.02f) {
+        float sd = fmaf(delta * d2, (float)(-1.0 / 6.0), delta);
+        float cd = fmaf(d2, fmaf(d2, (float)(1.0 / 24.0), -0.5f), 1.0f);
+        *st = fmaf(st0, cd, ct0 * sd);
+        *ct = fmaf(ct0, cd, -(st0 * sd));
+        return true;
+    }
     float ps = fmaf(d2, (float)(-1.0 / 5040.0), (float)(1.0 / 120.0));
     ps = fmaf(d2, ps, (float)(-1.0 / 6.0));
     float sd = fmaf(delta * d2, ps, delta);
@@ -553,11 +561,37 @@ template <typename R> __device__ __forceinline__ float k_drift(const KLane<R>& l
     return (float)(gmax(l.gauge, last) / l.scale);
 }
 
-template <typename R> __device__ __forceinline__ V3<R> k_position(const KLane<R>& l) {
+template <typename R> __device__ __forceinline__ V3<R> k_position(const KLane<R>& l, R* sp_out = nullptr,
+                                                                 R* cp_out = nullptr) {
     R sp, cp;
     fast_sincos(l.s.ph, &sp, &cp);
+    if (sp_out) *sp_out = sp;
+    if (cp_out) *cp_out = cp;
     R radial = asqrt(fmaT(l.s.r, l.s.r, l.k.a2));
     return v3<R>(radial * l.st * cp, radial * l.st * sp, l.s.r * l.ct);
+}
+
+// Direction of travel against the spherical frame (Kerr.h:158-173) from the
+// lane's state, with the sines and cosines the step already has and
+// reciprocals in place of the divides.
+template <typename R> __device__ __forceinline__ V3<R> k_direction(const KLane<R>& l, R sp, R cp) {
+    const KConst<R>& k = l.k;
+    const R r = l.s.r, st = l.st, ct = l.ct;
+    const R delta = fmaT(r, r - R(2), k.a2);
+    const R inv_sigma = rcp(fmaT(k.a2, ct * ct, r * r));
+    R inv_sin2, inv_sc;
+    k_sin_inverses(st, &inv_sin2, &inv_sc);
+    const R p = fmaT(r * r + k.a2, k.E, -k.aL);
+    const R rdot = delta * l.s.pr * inv_sigma;
+    const R r_thdot = r * l.s.pt * inv_sigma;
+    const R r_st_phdot = r * st * ((fmaT(k.a, p * rcp(delta), k.L * inv_sin2) - k.aE) * inv_sigma);
+    // rdot rhat + r thdot thhat + r sin phdot phhat, with rhat = (st cp, st sp, ct),
+    // thhat = (ct cp, ct sp, -st), phhat = (-sp, cp, 0).
+    const R in_plane = fmaT(rdot, st, r_thdot * ct);  // along (cp, sp, 0)
+    V3<R> local = v3<R>(fmaT(in_plane, cp, -r_st_phdot * sp), fmaT(in_plane, sp, r_st_phdot * cp),
+                        fmaT(rdot, ct, -r_thdot * st));
+    R len2 = dot(local, local);
+    return len2 > R(0) ? local * rsqrtT(len2) : v3<R>(st * cp, st * sp, ct);
 }
 
 // kerrLaunch (Kerr.h:110-148) into a lane.
@@ -607,7 +641,8 @@ __device__ __forceinline__ bool k_step(KLane<R>& l, const MarchUniforms& u, cuda
     comp_addT<Comp>(l.s.pt, l.c.pt, inc.pt);
     l.steps += 1u;
     fast_sincos(l.s.th, &l.st, &l.ct);
-    V3<R> position = k_position(l);
+    R sp, cp;
+    V3<R> position = k_position(l, &sp, &cp);
     V3<R> d = position - l.previous;
     float path = (float)asqrt(dot(d, d));
     l.travelled += path;
@@ -620,9 +655,8 @@ __device__ __forceinline__ bool k_step(KLane<R>& l, const MarchUniforms& u, cuda
     if (gather && in_slab(pf, u.volumeHalfExtent) && l.transmittance > 0.004f) {
         R sigma = fmaT(l.k.a2, l.ct * l.ct, l.s.r * l.s.r);
         float fk = (float)(R(1) - R(2) * l.s.r * rcp(sigma));
-        KerrState<R> ks{l.s.r, l.s.th, l.s.ph, l.s.pr, l.s.pt, l.k.E, l.k.L};
-        float3 dir = to_float3(kerr_direction(l.k.a, ks));
-        gather_sample(gather_view(u, em, vel), pf, fmaxf(fk, 0.0f), dir, path, l.travelled, l.color,
+        auto dir = [&] { return to_float3(k_direction(l, sp, cp)); };
+        gather_sample_with(gather_view(u, em, vel), pf, fmaxf(fk, 0.0f), dir, path, l.travelled, l.color,
                       l.transmittance, l.weighted_depth, l.depth_weight, l.samples);
     }
     l.previous = position;

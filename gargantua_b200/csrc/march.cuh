@@ -45,13 +45,14 @@ struct MarchResult {
     uint32_t samples;  // in-slab gather evaluations
 };
 
-// x += y with the error word e carried: TwoSum(x, y + e).
+// x += y with the error word e carried: Fast2Sum(x, y + e). The error word
+// is exact when |x| >= |y + e|, which holds for every state word except in
+// the step where a momentum or angle crosses zero; there the sum is still
+// correctly rounded and only that step's error word is approximate.
 __device__ __forceinline__ void comp_add(float& x, float& e, float y) {
     float b = __fadd_rn(y, e);
     float t = __fadd_rn(x, b);
-    float bp = __fsub_rn(t, x);
-    float ap = __fsub_rn(t, bp);
-    e = __fadd_rn(__fsub_rn(x, ap), __fsub_rn(b, bp));
+    e = __fsub_rn(b, __fsub_rn(t, x));
     x = t;
 }
 
@@ -83,15 +84,18 @@ __device__ __forceinline__ GatherView gather_view(const MarchUniforms& u, cudaTe
 }
 
 // Gather one in-slab sample into the running colour (march.metal:81-102).
-__device__ __forceinline__ void gather_sample(const GatherView& gv, float3 position, float f, float3 direction,
-                                              float path, float travelled, float3& color, float& transmittance,
-                                              float& weighted_depth, float& depth_weight, uint32_t& samples) {
+// The photon's direction is needed only for the redshift of a sample that
+// holds gas, so it is passed as a function evaluated there.
+template <typename Direction>
+__device__ __forceinline__ void gather_sample_with(const GatherView& gv, float3 position, float f, Direction direction,
+                                                   float path, float travelled, float3& color, float& transmittance,
+                                                   float& weighted_depth, float& depth_weight, uint32_t& samples) {
     samples += 1u;
     Sample s = sample_volume(position, gv.half_extent, gv.emission, gv.velocity);
     if (s.density > 0.0f) {
         float g3 = 1.0f;
         if (gv.redshift != 0u) {
-            float g = redshift_factor(f, direction, s.velocity);
+            float g = redshift_factor(f, direction(), s.velocity);
             float gravity = sqrtf(fmaxf(f, 0.0f));
             float bulk = fminf(s.density / BEAMING_DENSITY_FLOOR, 1.0f);
             float gr3 = gravity * gravity * gravity;
@@ -106,6 +110,13 @@ __device__ __forceinline__ void gather_sample(const GatherView& gv, float3 posit
         depth_weight += weight;
         transmittance *= 1.0f - alpha;
     }
+}
+
+__device__ __forceinline__ void gather_sample(const GatherView& gv, float3 position, float f, float3 direction,
+                                              float path, float travelled, float3& color, float& transmittance,
+                                              float& weighted_depth, float& depth_weight, uint32_t& samples) {
+    gather_sample_with(gv, position, f, [&] { return direction; }, path, travelled, color, transmittance,
+                       weighted_depth, depth_weight, samples);
 }
 
 __device__ __forceinline__ bool in_slab(float3 q, float half_extent) {
