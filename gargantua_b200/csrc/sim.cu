@@ -39,7 +39,18 @@ __device__ __forceinline__ float disk_shape_f(float r) {
     return gg_pow34f(x) * gg_pow14f(torque);
 }
 
-__device__ __forceinline__ float len3(float x, float y, float z) { return sqrtf(x * x + y * y + z * z); }
+__device__ __forceinline__ float square3(float x, float y, float z) { return x * x + y * y + z * z; }
+__device__ __forceinline__ float len3(float x, float y, float z) { return sqrtf(square3(x, y, z)); }
+
+// The step's two tests of a length against a limit, made on the squared
+// length: sqrt rounds correctly and monotonically, so sqrt(s) > 12 exactly
+// when s > 144 (no float lies between 144 and (12 + half an ulp)^2), and
+// sqrt(s) < 2.02f exactly when s < 4.0803995f (bits 0x408292a2, the least
+// float whose square root rounds to 2.02f or above). Both bounds were found
+// by testing every float near the squares; a CPU test repeats that search.
+constexpr float kPlungeSpeedSquared = 144.0f;
+constexpr uint32_t kCaptureClosestSquaredBits = 0x408292a2u;
+static_assert(PLUNGE_SPEED_LIMIT == 12.0f && R_CAPTURE == 2.02f, "the squared bounds belong to these limits");
 
 // spawn (sim.metal:6-34): event 0 seeds from the steady profile, later
 // events respawn into the feeding annulus. With a second seeding table
@@ -112,9 +123,10 @@ __global__ void __launch_bounds__(256) step_kernel(SimArgs a) {
     float4 v = a.vel[i];
     float px = p.x, py = p.y, pz = p.z;
     float vx = v.x, vy = v.y, vz = v.z;
+    const float capture_squared = __uint_as_float(kCaptureClosestSquaredBits);
+    float r = len3(px, py, pz);  // |x| at the start of each substep
 #pragma unroll
     for (uint32_t s = 0; s < SIM_SUBSTEPS; ++s) {
-        float r = len3(px, py, pz);
         float k = -potential_gradient(r, u.potential) / r;
         float omega = circular_speed(r, u.potential) / r;
         vx = vx + px * k * u.dt;
@@ -133,16 +145,18 @@ __global__ void __launch_bounds__(256) step_kernel(SimArgs a) {
         float bt = bx * tx + by * ty + bz * tz;
         float tt = tx * tx + ty * ty + tz * tz;
         float along = fminf(fmaxf(-bt / fmaxf(tt, 1e-12f), 0.0f), 1.0f);
-        float closest = len3(bx + along * tx, by + along * ty, bz + along * tz);
-        if (closest < R_CAPTURE || r > R_ESCAPE || len3(vx, vy, vz) > PLUNGE_SPEED_LIMIT) {
+        // closest < R_CAPTURE and |v| > PLUNGE_SPEED_LIMIT, on the squares
+        float closest_squared = square3(bx + along * tx, by + along * ty, bz + along * tz);
+        if (closest_squared < capture_squared || r > R_ESCAPE || square3(vx, vy, vz) > kPlungeSpeedSquared) {
             float4 np, nv;
             spawn(a.first_index + i, __float_as_uint(v.w) + 1u, a, false, np, nv);
             px = np.x; py = np.y; pz = np.z;
             vx = nv.x; vy = nv.y; vz = nv.z;
             v.w = nv.w;
+            r = len3(px, py, pz);
         }
     }
-    float t = u.temperatureScale * disk_shape_f(len3(px, py, pz));
+    float t = u.temperatureScale * disk_shape_f(r);
     a.pos[i] = make_float4(px, py, pz, t);
     a.vel[i] = make_float4(vx, vy, vz, v.w);
 }
