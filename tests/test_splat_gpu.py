@@ -70,10 +70,10 @@ def test_edge_particles_deposit_like_the_reference(ctx):
         assert np.array_equal(em, rem) and np.array_equal(mo, rmo) and np.array_equal(ma, rma)
 
 
-def test_resolve_is_bit_exact_and_clears_the_sums(ctx, settled):
+@pytest.mark.parametrize("size", [32, 96, 30, 33])  # whole and partial 32 x 8 blocks
+def test_resolve_is_bit_exact_and_clears_the_sums(ctx, settled, size):
     import gargantua_b200 as g
 
-    size = 32
     vol = g.Volume(ctx, size)
     vol.bin(settled, exact=True, frame=0)
     em, mo, ma = vol.read_sums()
