@@ -56,9 +56,9 @@ STREAM_LENGTH = 512
 FLOPS_SCHWARZSCHILD_STEP = 192  # RK4 165 + position 14 + step policy 3 + path 10
 FLOPS_KERR_STEP = 515           # RK4 436 + step policy, position, path, Carter and null gauges 79
 FLOPS_SAMPLE = 111              # in-slab gather 67 + static-observer direction 44
-# DRAM bytes of one serve_kerr_kernel launch (ncu, 1920x1080 4096-step Kerr still): the march
-# reads only its descriptors and tables from HBM; pixels stay in L2 until the copy-out.
-SERVE_KERR_TRAFFIC_BYTES = 8408320
+# DRAM bytes of one serve_kerr_chunks_kernel launch (ncu, 1920x1080 4096-step Kerr still): the
+# march reads only its descriptors and tables from HBM; pixels stay in L2 until the copy-out.
+SERVE_KERR_TRAFFIC_BYTES = 8403456
 
 
 def make_stream(seed: int, count: int = STREAM_LENGTH):
@@ -647,10 +647,11 @@ def main():
                 "d2h_bytes_per_step": int(d2h / max(args.steps, 1))},
         "roofline": {"bound": "fp32", "achieved": achieved, "peak": peak, "unit": "TFLOP/s",
                      "frac": achieved / peak, "traffic": SERVE_KERR_TRAFFIC_BYTES,
-                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one serve_kerr_kernel "
-                                       "launch serving a 1920x1080 4096-step Kerr still",
+                     "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum of one "
+                                       "serve_kerr_chunks_kernel launch serving a 1920x1080 4096-step Kerr still",
                      "peak_source": "measured FP32 FMA microbenchmark (gg_measure_fp32_peak) on this GPU",
-                     "kernel": "serve_kerr_kernel + serve_schwarzschild_kernel (persistent, work-stealing)",
+                     "kernel": "serve_kerr_chunks_kernel + serve_schwarzschild_chunks_kernel (persistent, "
+                               "work-stealing)",
                      "device_busy_fraction": busy / max(span, 1e-12)},
         "cpu_baseline": cpu,
         "passes": passes,
