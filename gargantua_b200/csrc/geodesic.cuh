@@ -271,11 +271,15 @@ struct Sample {
 };
 
 // Two trilinear half4 fetches, zero outside the cube (march.metal:15-27).
-__device__ __forceinline__ Sample sample_volume(float3 p, float half_extent, cudaTextureObject_t em, cudaTextureObject_t vel) {
+__device__ __forceinline__ float3 volume_coordinates(float3 p, float half_extent) {
     float inv = 1.0f / (2.0f * half_extent);
-    float ux = (p.x + half_extent) * inv, uy = (p.y + half_extent) * inv, uz = (p.z + half_extent) * inv;
-    float4 e = tex3D<float4>(em, ux, uy, uz);
-    float4 v = tex3D<float4>(vel, ux, uy, uz);
+    return make_float3((p.x + half_extent) * inv, (p.y + half_extent) * inv, (p.z + half_extent) * inv);
+}
+
+__device__ __forceinline__ Sample sample_volume(float3 p, float half_extent, cudaTextureObject_t em, cudaTextureObject_t vel) {
+    float3 c = volume_coordinates(p, half_extent);
+    float4 e = tex3D<float4>(em, c.x, c.y, c.z);
+    float4 v = tex3D<float4>(vel, c.x, c.y, c.z);
     Sample s;
     s.emission = make_float3(e.x, e.y, e.z);
     s.density = e.w;

@@ -98,36 +98,11 @@ __device__ __forceinline__ void fast_sincos(double x, double* s_out, double* c_o
     *c_out = c;
 }
 
-// Reciprocal: FP32 within one ulp (PTX rcp.approx); FP64 from the
-// approximate reciprocal refined by two Newton steps y += y (1 - x y).
-__device__ __forceinline__ float rcp(float x) {
-    float y;
-    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
-    return y;
-}
-
-__device__ __forceinline__ double rcp(double x) {
-    double y;
-    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
-    double e = fma(-x, y, 1.0);
-    y = fma(y, e, y);
-    e = fma(-x, y, 1.0);
-    return fma(y, e, y);
-}
-
 __device__ __forceinline__ float fmaT(float a, float b, float c) { return fmaf(a, b, c); }
 __device__ __forceinline__ double fmaT(double a, double b, double c) { return fma(a, b, c); }
 __device__ __forceinline__ float rsqrtT(float x) { return rsqrtf(x); }
 __device__ __forceinline__ double rsqrtT(double x) { return rcp(sqrt(x)); }
 
-// Square root for lengths that feed only path lengths and sample positions:
-// FP32 from sqrt.approx (relative error below 2^-22), FP64 exact.
-__device__ __forceinline__ float asqrt(float x) {
-    float y;
-    asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
-    return y;
-}
-__device__ __forceinline__ double asqrt(double x) { return sqrt(x); }
 
 // x += y. Compensated FP32 carries the rounding error in e (TwoSum,
 // march.cuh); plain FP32 and FP64 add directly and leave e at zero.
@@ -286,7 +261,7 @@ __device__ __forceinline__ bool s_step(SLane<R>& l, const MarchUniforms& u, cuda
     float3 pf = to_float3(position);
     if (gather && in_slab(pf, u.volumeHalfExtent) && l.transmittance > 0.004f) {
         float f = (float)fmaT(R(-2), rcp(l.s.r), R(1));
-        gather_sample_with(gather_view(u, em, vel), pf, f, [&] { return to_float3(s_direction(l, sn, cs)); }, path,
+        gather_sample_with<true>(gather_view(u, em, vel), pf, f, [&] { return to_float3(s_direction(l, sn, cs)); }, path,
                            l.travelled, l.color, l.transmittance, l.weighted_depth, l.depth_weight, l.samples);
     }
     l.previous = position;
@@ -656,7 +631,7 @@ __device__ __forceinline__ bool k_step(KLane<R>& l, const MarchUniforms& u, cuda
         R sigma = fmaT(l.k.a2, l.ct * l.ct, l.s.r * l.s.r);
         float fk = (float)(R(1) - R(2) * l.s.r * rcp(sigma));
         auto dir = [&] { return to_float3(k_direction(l, sp, cp)); };
-        gather_sample_with(gather_view(u, em, vel), pf, fmaxf(fk, 0.0f), dir, path, l.travelled, l.color,
+        gather_sample_with<true>(gather_view(u, em, vel), pf, fmaxf(fk, 0.0f), dir, path, l.travelled, l.color,
                       l.transmittance, l.weighted_depth, l.depth_weight, l.samples);
     }
     l.previous = position;

@@ -71,6 +71,32 @@ __device__ __forceinline__ void advance(RayState<R>& s, RayState<R>& c, R h) {
     }
 }
 
+// Reciprocal: FP32 within one ulp (PTX rcp.approx); FP64 from the
+// approximate reciprocal refined by two Newton steps y += y (1 - x y).
+__device__ __forceinline__ float rcp(float x) {
+    float y;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+
+__device__ __forceinline__ double rcp(double x) {
+    double y;
+    asm("rcp.approx.ftz.f64 %0, %1;" : "=d"(y) : "d"(x));
+    double e = fma(-x, y, 1.0);
+    y = fma(y, e, y);
+    e = fma(-x, y, 1.0);
+    return fma(y, e, y);
+}
+
+// Square root for lengths that feed only path lengths and sample positions:
+// FP32 from sqrt.approx (relative error below 2^-22), FP64 exact.
+__device__ __forceinline__ float asqrt(float x) {
+    float y;
+    asm("sqrt.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ double asqrt(double x) { return sqrt(x); }
+
 struct GatherView {
     cudaTextureObject_t emission;
     cudaTextureObject_t velocity;
@@ -86,22 +112,53 @@ __device__ __forceinline__ GatherView gather_view(const MarchUniforms& u, cudaTe
 // Gather one in-slab sample into the running colour (march.metal:81-102).
 // The photon's direction is needed only for the redshift of a sample that
 // holds gas, so it is passed as a function evaluated there.
-template <typename Direction>
+//
+// Fast (the lanes: served, plain and compensated marches) evaluates the
+// redshift and opacity with hardware approximations where the reference's
+// kernel calls precise functions: tanh from one exponential, tanh x = 1 -
+// 2 / (e^2x + 1) (absolute error near 1e-7), the exponentials, reciprocals
+// and square roots approximate (relative errors of a few 1e-7). Without
+// Fast (the per-request kernel as written) the arithmetic is the
+// reference's. The texture coordinates are the reference's in both.
+template <bool Fast, typename Direction>
 __device__ __forceinline__ void gather_sample_with(const GatherView& gv, float3 position, float f, Direction direction,
                                                    float path, float travelled, float3& color, float& transmittance,
                                                    float& weighted_depth, float& depth_weight, uint32_t& samples) {
     samples += 1u;
-    Sample s = sample_volume(position, gv.half_extent, gv.emission, gv.velocity);
+    // sampleVolume (march.metal:15-27); the velocity texel is fetched only
+    // where the redshift reads it (gas present, redshift on).
+    const float3 c = volume_coordinates(position, gv.half_extent);
+    const float4 e = tex3D<float4>(gv.emission, c.x, c.y, c.z);
+    Sample s;
+    s.emission = make_float3(e.x, e.y, e.z);
+    s.density = e.w;
     if (s.density > 0.0f) {
         float g3 = 1.0f;
         if (gv.redshift != 0u) {
-            float g = redshift_factor(f, direction(), s.velocity);
-            float gravity = sqrtf(fmaxf(f, 0.0f));
-            float bulk = fminf(s.density / BEAMING_DENSITY_FLOOR, 1.0f);
+            const float4 v = tex3D<float4>(gv.velocity, c.x, c.y, c.z);
+            s.velocity = make_float3(v.x, v.y, v.z);
+            float g, gravity, bulk;
+            if constexpr (Fast) {
+                // redshiftFactor (Geodesic.h:225-236) as redshift_factor below.
+                const float3 gas = s.velocity;
+                const float magnitude = asqrt(dot3(gas, gas));
+                const float speed = fminf(magnitude, 8.0f);
+                const float beta =
+                    GAS_SPEED_CEILING * (1.0f - 2.0f * rcp(__expf(speed * (2.0f / GAS_SPEED_CEILING)) + 1.0f));
+                const float scale = magnitude > 0.0f ? beta * rcp(magnitude) : 0.0f;
+                gravity = asqrt(fmaxf(f, 0.0f));
+                g = gravity * asqrt(1.0f - beta * beta) * rcp(fmaf(dot3(direction(), gas), scale, 1.0f));
+                bulk = fminf(s.density * (1.0f / BEAMING_DENSITY_FLOOR), 1.0f);
+            } else {
+                g = redshift_factor(f, direction(), s.velocity);
+                gravity = sqrtf(fmaxf(f, 0.0f));
+                bulk = fminf(s.density / BEAMING_DENSITY_FLOOR, 1.0f);
+            }
             float gr3 = gravity * gravity * gravity;
             g3 = gr3 + (g * g * g - gr3) * bulk;
         }
-        float alpha = 1.0f - expf(-gv.opacity * s.density * path);
+        float extinction = -gv.opacity * s.density * path;
+        float alpha = 1.0f - (Fast ? __expf(extinction) : expf(extinction));
         float k = transmittance * g3 * path;
         float3 contribution = make_float3(s.emission.x * k, s.emission.y * k, s.emission.z * k);
         color = color + contribution;
@@ -115,8 +172,8 @@ __device__ __forceinline__ void gather_sample_with(const GatherView& gv, float3 
 __device__ __forceinline__ void gather_sample(const GatherView& gv, float3 position, float f, float3 direction,
                                               float path, float travelled, float3& color, float& transmittance,
                                               float& weighted_depth, float& depth_weight, uint32_t& samples) {
-    gather_sample_with(gv, position, f, [&] { return direction; }, path, travelled, color, transmittance,
-                       weighted_depth, depth_weight, samples);
+    gather_sample_with<false>(gv, position, f, [&] { return direction; }, path, travelled, color, transmittance,
+                              weighted_depth, depth_weight, samples);
 }
 
 __device__ __forceinline__ bool in_slab(float3 q, float half_extent) {
