@@ -1,6 +1,6 @@
 """The 11 goldens against the device, mirroring `gargantua validate`
 (Sources/Gargantua/Validation/Validate.swift:17-374) function by function.
-The FP64 oracle (oracle/) is the judge where the reference's is."""
+The FP64 oracle (oracle/) decides where the reference's Swift oracle does."""
 import math
 import os
 
