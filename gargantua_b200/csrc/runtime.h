@@ -137,8 +137,9 @@ struct gg_volume {
     // (0: direct global atomics) and particles per deposit work item.
     uint32_t brick_edge[2] = {0u, 8u};    // [stochastic, exact]; set per size by gg_volume_create
     uint32_t brick_chunk[2] = {0u, 1024u};
-    void* brick_scratch = nullptr;  // counts, offsets, cursor, items, sorted slots, keys
+    void* brick_scratch = nullptr;  // counts, cursor, offsets, items, sorted slots, keys
     uint64_t brick_scratch_capacity = 0;
+    bool brick_counts_zero = false;  // the counts region holds zeros (the count pass re-zeroes it)
 };
 
 struct gg_targets {

@@ -158,7 +158,7 @@ struct BrickArgs {
     uint32_t per_axis;   // ceil(n / B)
     uint32_t bricks;     // per_axis^3
     uint32_t chunk;      // particles per deposit work item
-    uint32_t* counts;    // [bricks]
+    uint32_t* counts;    // [kMaxBricks + 1]: counts, then the count pass's finished-block counter; zero between calls
     uint32_t* offsets;   // [bricks + 1], exclusive scan of counts
     uint32_t* cursor;    // [bricks], reservation cursor
     uint32_t* items;     // [bricks + 1], exclusive scan of ceil(count / chunk)
@@ -170,8 +170,76 @@ __device__ __forceinline__ uint32_t brick_of(const Footprint& f, const BrickArgs
     return ((uint32_t)f.lz / a.edge * a.per_axis + (uint32_t)f.ly / a.edge) * a.per_axis + (uint32_t)f.lx / a.edge;
 }
 
+// Inclusive sum over the warp of a value per lane (shuffle scan).
+__device__ __forceinline__ uint32_t warp_inclusive(uint32_t v, uint32_t lane) {
+#pragma unroll
+    for (uint32_t off = 1; off < 32u; off <<= 1) {
+        uint32_t u = __shfl_up_sync(0xffffffffu, v, off);
+        if (lane >= off) v += u;
+    }
+    return v;
+}
+
+// Exclusive scans of the brick counts (offsets, cursor) and of their work
+// items ceil(count / chunk) (items), by one block of kBrickBlock threads:
+// each thread scans a contiguous run of bricks, the per-thread totals are
+// scanned with warp shuffles and one pass over the warp totals. The counts
+// are read from L2 (other blocks added them) and zeroed behind the read, so
+// they start at zero at the next call.
+__device__ void scan_bricks(const BrickArgs& a) {
+    constexpr uint32_t kWarps = kBrickBlock / 32u;
+    __shared__ uint32_t warp_p[kWarps], warp_i[kWarps];
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
+    const uint32_t per = (a.bricks + kBrickBlock - 1u) / kBrickBlock;
+    const uint32_t b0 = min(threadIdx.x * per, a.bricks), b1 = min(b0 + per, a.bricks);
+    uint32_t sp = 0, si = 0;
+#pragma unroll 4
+    for (uint32_t b = b0; b < b1; ++b) {
+        const uint32_t c = __ldcg(a.counts + b);
+        sp += c;
+        si += (c + a.chunk - 1u) / a.chunk;
+    }
+    const uint32_t ip = warp_inclusive(sp, lane), ii = warp_inclusive(si, lane);
+    if (lane == 31u) {
+        warp_p[warp] = ip;
+        warp_i[warp] = ii;
+    }
+    __syncthreads();
+    if (warp == 0) {
+        const uint32_t wp = warp_inclusive(lane < kWarps ? warp_p[lane] : 0u, lane);
+        const uint32_t wi = warp_inclusive(lane < kWarps ? warp_i[lane] : 0u, lane);
+        if (lane < kWarps) {
+            warp_p[lane] = wp;  // inclusive totals through warp `lane`
+            warp_i[lane] = wi;
+        }
+    }
+    __syncthreads();
+    uint32_t op = (warp ? warp_p[warp - 1] : 0u) + ip - sp;  // exclusive prefix of this thread's run
+    uint32_t oi = (warp ? warp_i[warp - 1] : 0u) + ii - si;
+#pragma unroll 4
+    for (uint32_t b = b0; b < b1; ++b) {
+        const uint32_t c = __ldcg(a.counts + b);
+        a.counts[b] = 0u;
+        a.offsets[b] = op;
+        a.cursor[b] = op;
+        a.items[b] = oi;
+        op += c;
+        oi += (c + a.chunk - 1u) / a.chunk;
+    }
+    if (threadIdx.x == kBrickBlock - 1u) {
+        a.offsets[a.bricks] = warp_p[kWarps - 1];
+        a.items[a.bricks] = warp_i[kWarps - 1];
+        a.counts[kMaxBricks] = 0u;  // the finished-block counter, for the next call
+    }
+}
+
+// Each block histograms its particles' bricks in shared memory and adds the
+// histogram to the counts; the block that finishes last (the counter at
+// counts[kMaxBricks], after a fence, as in a threadfence reduction; nothing
+// waits) then scans them.
 __global__ void __launch_bounds__(kBrickBlock) brick_count_kernel(BrickArgs a) {
     extern __shared__ uint32_t hist[];
+    __shared__ bool last;
     for (uint32_t b = threadIdx.x; b < a.bricks; b += blockDim.x) hist[b] = 0u;
     __syncthreads();
     const uint32_t begin = blockIdx.x * kBrickParticlesPerBlock;
@@ -188,58 +256,13 @@ __global__ void __launch_bounds__(kBrickBlock) brick_count_kernel(BrickArgs a) {
     __syncthreads();
     for (uint32_t b = threadIdx.x; b < a.bricks; b += blockDim.x)
         if (hist[b]) atomicAdd(&a.counts[b], hist[b]);
-}
-
-// Inclusive sum over the warp of a value per lane (shuffle scan).
-__device__ __forceinline__ uint32_t warp_inclusive(uint32_t v, uint32_t lane) {
-#pragma unroll
-    for (uint32_t off = 1; off < 32u; off <<= 1) {
-        uint32_t u = __shfl_up_sync(0xffffffffu, v, off);
-        if (lane >= off) v += u;
-    }
-    return v;
-}
-
-// One block of 1024 threads: each thread scans a contiguous run of bricks;
-// the per-thread totals are scanned with warp shuffles and one pass over the
-// 32 warp totals.
-__global__ void __launch_bounds__(1024) brick_scan_kernel(BrickArgs a) {
-    __shared__ uint32_t warp_p[32], warp_i[32];
-    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-    const uint32_t per = (a.bricks + blockDim.x - 1) / blockDim.x;
-    const uint32_t b0 = threadIdx.x * per, b1 = min(b0 + per, a.bricks);
-    uint32_t sp = 0, si = 0;
-    for (uint32_t b = b0; b < b1; ++b) {
-        const uint32_t c = a.counts[b];
-        sp += c;
-        si += (c + a.chunk - 1u) / a.chunk;
-    }
-    const uint32_t ip = warp_inclusive(sp, lane), ii = warp_inclusive(si, lane);
-    if (lane == 31u) {
-        warp_p[warp] = ip;
-        warp_i[warp] = ii;
-    }
+    __threadfence();
     __syncthreads();
-    if (warp == 0) {
-        const uint32_t wp = warp_inclusive(warp_p[lane], lane), wi = warp_inclusive(warp_i[lane], lane);
-        warp_p[lane] = wp;  // inclusive totals through warp `lane`
-        warp_i[lane] = wi;
-    }
+    if (threadIdx.x == 0) last = atomicAdd(&a.counts[kMaxBricks], 1u) == gridDim.x - 1u;
     __syncthreads();
-    uint32_t op = (warp ? warp_p[warp - 1] : 0u) + ip - sp;  // exclusive prefix of this thread's run
-    uint32_t oi = (warp ? warp_i[warp - 1] : 0u) + ii - si;
-    for (uint32_t b = b0; b < b1; ++b) {
-        const uint32_t c = a.counts[b];
-        a.offsets[b] = op;
-        a.cursor[b] = op;
-        a.items[b] = oi;
-        op += c;
-        oi += (c + a.chunk - 1u) / a.chunk;
-    }
-    if (threadIdx.x == blockDim.x - 1) {
-        a.offsets[a.bricks] = warp_p[31];
-        a.items[a.bricks] = warp_i[31];
-    }
+    if (!last) return;
+    __threadfence();
+    scan_bricks(a);
 }
 
 __global__ void __launch_bounds__(kBrickBlock) brick_scatter_kernel(BrickArgs a) {
@@ -485,10 +508,19 @@ static int splat_bin_shaped(gg_particles* ps, gg_volume* vol, const SplatUniform
     GG_CHECK(check_shape(vol, edge, chunk));
     const uint32_t per = bricks_per_axis(vol->size, edge);
     const uint32_t bricks = per * per * per;
-    const uint64_t words = align256(4ull * bricks) * 2u + align256(4ull * (bricks + 1u)) * 2u;
+    // counts (a fixed kMaxBricks + 1 words, whatever the shape, so that the
+    // zeros the scan leaves behind stay counts), cursor, offsets, items,
+    // sorted slots, keys.
+    const uint64_t counts_bytes = align256(4ull * (kMaxBricks + 1u));
+    const uint64_t words = counts_bytes + align256(4ull * bricks) + align256(4ull * (bricks + 1u)) * 2u;
     const uint64_t bytes = words + 2u * align256(4ull * ps->count);
+    const uint64_t capacity_before = vol->brick_scratch_capacity;  // changes when the scratch is reallocated
     GG_CHECK(gg::ensure_capacity(ctx, &vol->brick_scratch, &vol->brick_scratch_capacity, bytes, "splat bricks"));
     char* base = static_cast<char*>(vol->brick_scratch);
+    if (vol->brick_scratch_capacity != capacity_before || !vol->brick_counts_zero) {
+        GG_CUDA(cudaMemsetAsync(base, 0, counts_bytes, ctx->stream), "brick counts");
+        vol->brick_counts_zero = true;
+    }
     BrickArgs a;
     a.pos = ps->pos;
     a.vel = ps->vel;
@@ -500,20 +532,20 @@ static int splat_bin_shaped(gg_particles* ps, gg_volume* vol, const SplatUniform
     a.bricks = bricks;
     a.chunk = chunk;
     a.counts = reinterpret_cast<uint32_t*>(base);
-    a.cursor = reinterpret_cast<uint32_t*>(base + align256(4ull * bricks));
-    a.offsets = reinterpret_cast<uint32_t*>(base + 2u * align256(4ull * bricks));
-    a.items = reinterpret_cast<uint32_t*>(base + 2u * align256(4ull * bricks) + align256(4ull * (bricks + 1u)));
+    a.cursor = reinterpret_cast<uint32_t*>(base + counts_bytes);
+    a.offsets = reinterpret_cast<uint32_t*>(base + counts_bytes + align256(4ull * bricks));
+    a.items = reinterpret_cast<uint32_t*>(base + counts_bytes + align256(4ull * bricks) + align256(4ull * (bricks + 1u)));
     a.sorted = reinterpret_cast<uint32_t*>(base + words);
     a.keys = reinterpret_cast<uint32_t*>(base + words + align256(4ull * ps->count));
-    GG_CUDA(cudaMemsetAsync(a.counts, 0, 4ull * bricks, ctx->stream), "brick counts");
     const int hist = (int)(4u * bricks);
     GG_CHECK(allow_shared((const void*)brick_count_kernel, hist, ctx->device, 0));
     GG_CHECK(allow_shared((const void*)brick_scatter_kernel, hist, ctx->device, 1));
     const uint32_t blocks = (ps->count + kBrickParticlesPerBlock - 1u) / kBrickParticlesPerBlock;
+    // A failed launch leaves the counts in an unknown state: clear them next time.
+    vol->brick_counts_zero = false;
     brick_count_kernel<<<blocks, kBrickBlock, hist, ctx->stream>>>(a);
     GG_CHECK(gg::launch_status("brick count"));
-    brick_scan_kernel<<<1, 1024, 0, ctx->stream>>>(a);
-    GG_CHECK(gg::launch_status("brick scan"));
+    vol->brick_counts_zero = true;
     brick_scatter_kernel<<<blocks, kBrickBlock, hist, ctx->stream>>>(a);
     GG_CHECK(gg::launch_status("brick scatter"));
     // Work items number at most count / chunk + one per non-empty brick.
