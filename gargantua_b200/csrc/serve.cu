@@ -295,11 +295,16 @@ __global__ void __launch_bounds__(kServeThreads) serve_kerr_kernel(WaveArgs a) {
     serve_queue<1>(a, threadIdx.x & 31u);
 }
 
-__global__ void __launch_bounds__(kServeThreads) serve_schwarzschild_chunks_kernel(WaveArgs a) {
+// The chunk kernels are held to 5 blocks per SM (at most 102 registers; they
+// need 96 without spilling): 20 warps per SM instead of 16 served the stream
+// 1.7 % faster than the 119 registers the compiler picks unbounded.
+constexpr int kServeChunkBlocksPerSM = 5;
+
+__global__ void __launch_bounds__(kServeThreads, kServeChunkBlocksPerSM) serve_schwarzschild_chunks_kernel(WaveArgs a) {
     serve_chunks<0>(a, threadIdx.x & 31u);
 }
 
-__global__ void __launch_bounds__(kServeThreads) serve_kerr_chunks_kernel(WaveArgs a) {
+__global__ void __launch_bounds__(kServeThreads, kServeChunkBlocksPerSM) serve_kerr_chunks_kernel(WaveArgs a) {
     serve_chunks<1>(a, threadIdx.x & 31u);
 }
 
