@@ -286,25 +286,26 @@ __device__ void serve_chunks(const WaveArgs& a, uint32_t lane) {
 }
 
 // One persistent kernel per metric and schedule; a wave runs the two
-// metrics side by side.
-__global__ void __launch_bounds__(kServeThreads) serve_schwarzschild_kernel(WaveArgs a) {
+// metrics side by side. All four are held to 5 blocks per SM (at most 102
+// registers; the step needs 96 without spilling): 20 warps per SM instead of
+// 16 served the stream 1.7 % faster than the 119 registers the compiler
+// picks unbounded, and compiling every schedule under the same bound keeps
+// their arithmetic, and so their pixels, identical.
+constexpr int kServeBlocksPerSM = 5;
+
+__global__ void __launch_bounds__(kServeThreads, kServeBlocksPerSM) serve_schwarzschild_kernel(WaveArgs a) {
     serve_queue<0>(a, threadIdx.x & 31u);
 }
 
-__global__ void __launch_bounds__(kServeThreads) serve_kerr_kernel(WaveArgs a) {
+__global__ void __launch_bounds__(kServeThreads, kServeBlocksPerSM) serve_kerr_kernel(WaveArgs a) {
     serve_queue<1>(a, threadIdx.x & 31u);
 }
 
-// The chunk kernels are held to 5 blocks per SM (at most 102 registers; they
-// need 96 without spilling): 20 warps per SM instead of 16 served the stream
-// 1.7 % faster than the 119 registers the compiler picks unbounded.
-constexpr int kServeChunkBlocksPerSM = 5;
-
-__global__ void __launch_bounds__(kServeThreads, kServeChunkBlocksPerSM) serve_schwarzschild_chunks_kernel(WaveArgs a) {
+__global__ void __launch_bounds__(kServeThreads, kServeBlocksPerSM) serve_schwarzschild_chunks_kernel(WaveArgs a) {
     serve_chunks<0>(a, threadIdx.x & 31u);
 }
 
-__global__ void __launch_bounds__(kServeThreads, kServeChunkBlocksPerSM) serve_kerr_chunks_kernel(WaveArgs a) {
+__global__ void __launch_bounds__(kServeThreads, kServeBlocksPerSM) serve_kerr_chunks_kernel(WaveArgs a) {
     serve_chunks<1>(a, threadIdx.x & 31u);
 }
 
@@ -778,6 +779,10 @@ static void worker_loop(gg_server* s) {
 
 }  // namespace gg
 
+namespace gg {
+void release_server_resources(gg_server* s);
+}
+
 using namespace gg;
 
 extern "C" {
@@ -788,7 +793,12 @@ GG_API int gg_server_create(gg_context* ctx, const gg_volume* vol, const gg_serv
     if (vol && vol->ctx != ctx) return gg::fail(GG_ERR_INVALID_ARGUMENT, "gg_server_create: volume from another context.");
     std::lock_guard<std::recursive_mutex> clock(ctx->mu);
     GG_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
-    std::unique_ptr<gg_server> s(new gg_server());
+    // Until it is handed out, a failure releases whatever was created.
+    auto discard = [](gg_server* p) {
+        gg::release_server_resources(p);
+        delete p;
+    };
+    std::unique_ptr<gg_server, decltype(discard)> s(new gg_server(), discard);
     s->ctx = ctx;
     s->vol = vol;
     if (config) s->cfg = *config;
@@ -887,14 +897,26 @@ GG_API void gg_server_destroy(gg_server* s) {
     }
     s->cv_work.notify_all();
     if (s->worker.joinable()) s->worker.join();
+    gg::release_server_resources(s);
+    s->ctx->used -= std::min(s->ctx->used, s->cfg.memory_bytes);
+    delete s;
+}
+
+}  // extern "C"
+
+namespace gg {
+
+// The device and host resources a server holds, whichever of them exist
+// (a server whose creation failed part way holds some).
+void release_server_resources(gg_server* s) {
     gg_context* ctx = s->ctx;
     cudaSetDevice(ctx->device);
     for (auto& w : s->slots) {
         if (w.stream) cudaStreamSynchronize(w.stream);
+        if (w.fp64) cudaStreamSynchronize(w.fp64);  // the FP64 pass reads the slot's flagged list
         if (w.graph) cudaGraphExecDestroy(w.graph);
         if (w.device) gg::device_free(ctx, w.device, s->slot_bytes);
         if (w.host) cudaFreeHost(w.host);
-        if (w.fp64) cudaStreamSynchronize(w.fp64);
         if (w.start) cudaEventDestroy(w.start);
         if (w.stop) cudaEventDestroy(w.stop);
         if (w.fork) cudaEventDestroy(w.fork);
@@ -904,19 +926,21 @@ GG_API void gg_server_destroy(gg_server* s) {
         if (w.fp64) cudaStreamDestroy(w.fp64);
         if (w.stream) cudaStreamDestroy(w.stream);
     }
-    cudaStreamSynchronize(s->copy);
-    cudaStreamSynchronize(s->build);
+    if (s->copy) cudaStreamSynchronize(s->copy);
+    if (s->build) cudaStreamSynchronize(s->build);
     for (auto& r : s->admitted) gg::release(s, *r);
-    cudaStreamSynchronize(s->copy);
-    ctx->used -= std::min(ctx->used, s->cfg.memory_bytes);
-    cudaEventDestroy(s->built);
-    cudaEventDestroy(s->origin);
-    cudaStreamDestroy(s->build);
-    cudaStreamDestroy(s->copy);
-    cudaStreamDestroy(s->plain);
+    if (s->copy) cudaStreamSynchronize(s->copy);
+    if (s->built) cudaEventDestroy(s->built);
+    if (s->origin) cudaEventDestroy(s->origin);
+    if (s->build) cudaStreamDestroy(s->build);
+    if (s->copy) cudaStreamDestroy(s->copy);
+    if (s->plain) cudaStreamDestroy(s->plain);
     if (s->pool) cudaMemPoolDestroy(s->pool);
-    delete s;
 }
+
+}  // namespace gg
+
+extern "C" {
 
 GG_API int gg_server_submit(gg_server* s, const gg_request* req, uint64_t* ticket) {
     if (!s || !req || !ticket) return gg::fail(GG_ERR_INVALID_ARGUMENT, "gg_server_submit needs a server, a request and a ticket.");

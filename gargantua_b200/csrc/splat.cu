@@ -158,6 +158,7 @@ struct BrickArgs {
     uint32_t per_axis;   // ceil(n / B)
     uint32_t bricks;     // per_axis^3
     uint32_t chunk;      // particles per deposit work item
+    uint32_t chunk_shift;  // log2(chunk) when chunk is a power of two, else 32
     uint32_t* counts;    // [kMaxBricks + 1]: counts, then the count pass's finished-block counter; zero between calls
     uint32_t* offsets;   // [bricks + 1], exclusive scan of counts
     uint32_t* cursor;    // [bricks], reservation cursor
@@ -180,12 +181,21 @@ __device__ __forceinline__ uint32_t warp_inclusive(uint32_t v, uint32_t lane) {
     return v;
 }
 
+// Work items of a brick of c particles: ceil(c / chunk), a shift when the
+// chunk is a power of two.
+__device__ __forceinline__ uint32_t brick_items(uint32_t c, const BrickArgs& a) {
+    return a.chunk_shift < 32u ? (c + a.chunk - 1u) >> a.chunk_shift : (c + a.chunk - 1u) / a.chunk;
+}
+
 // Exclusive scans of the brick counts (offsets, cursor) and of their work
-// items ceil(count / chunk) (items), by one block of kBrickBlock threads:
-// each thread scans a contiguous run of bricks, the per-thread totals are
-// scanned with warp shuffles and one pass over the warp totals. The counts
-// are read from L2 (other blocks added them) and zeroed behind the read, so
-// they start at zero at the next call.
+// items (items), by one block of kBrickBlock threads: each thread scans a
+// contiguous run of bricks, loading its counts kScanBatch at a time so the
+// loads are in flight together; the per-thread totals are scanned with warp
+// shuffles and one pass over the warp totals. The counts are read from L2
+// (other blocks added them) and zeroed behind the read, so they start at
+// zero at the next call.
+constexpr uint32_t kScanBatch = 16;
+
 __device__ void scan_bricks(const BrickArgs& a) {
     constexpr uint32_t kWarps = kBrickBlock / 32u;
     __shared__ uint32_t warp_p[kWarps], warp_i[kWarps];
@@ -193,11 +203,15 @@ __device__ void scan_bricks(const BrickArgs& a) {
     const uint32_t per = (a.bricks + kBrickBlock - 1u) / kBrickBlock;
     const uint32_t b0 = min(threadIdx.x * per, a.bricks), b1 = min(b0 + per, a.bricks);
     uint32_t sp = 0, si = 0;
-#pragma unroll 4
-    for (uint32_t b = b0; b < b1; ++b) {
-        const uint32_t c = __ldcg(a.counts + b);
-        sp += c;
-        si += (c + a.chunk - 1u) / a.chunk;
+    for (uint32_t b = b0; b < b1; b += kScanBatch) {
+        uint32_t c[kScanBatch];
+#pragma unroll
+        for (uint32_t j = 0; j < kScanBatch; ++j) c[j] = b + j < b1 ? __ldcg(a.counts + b + j) : 0u;
+#pragma unroll
+        for (uint32_t j = 0; j < kScanBatch; ++j) {
+            sp += c[j];
+            si += brick_items(c[j], a);
+        }
     }
     const uint32_t ip = warp_inclusive(sp, lane), ii = warp_inclusive(si, lane);
     if (lane == 31u) {
@@ -216,15 +230,20 @@ __device__ void scan_bricks(const BrickArgs& a) {
     __syncthreads();
     uint32_t op = (warp ? warp_p[warp - 1] : 0u) + ip - sp;  // exclusive prefix of this thread's run
     uint32_t oi = (warp ? warp_i[warp - 1] : 0u) + ii - si;
-#pragma unroll 4
-    for (uint32_t b = b0; b < b1; ++b) {
-        const uint32_t c = __ldcg(a.counts + b);
-        a.counts[b] = 0u;
-        a.offsets[b] = op;
-        a.cursor[b] = op;
-        a.items[b] = oi;
-        op += c;
-        oi += (c + a.chunk - 1u) / a.chunk;
+    for (uint32_t b = b0; b < b1; b += kScanBatch) {
+        uint32_t c[kScanBatch];
+#pragma unroll
+        for (uint32_t j = 0; j < kScanBatch; ++j) c[j] = b + j < b1 ? __ldcg(a.counts + b + j) : 0u;
+#pragma unroll
+        for (uint32_t j = 0; j < kScanBatch; ++j) {
+            if (b + j >= b1) break;
+            a.counts[b + j] = 0u;
+            a.offsets[b + j] = op;
+            a.cursor[b + j] = op;
+            a.items[b + j] = oi;
+            op += c[j];
+            oi += brick_items(c[j], a);
+        }
     }
     if (threadIdx.x == kBrickBlock - 1u) {
         a.offsets[a.bricks] = warp_p[kWarps - 1];
@@ -531,6 +550,10 @@ static int splat_bin_shaped(gg_particles* ps, gg_volume* vol, const SplatUniform
     a.per_axis = per;
     a.bricks = bricks;
     a.chunk = chunk;
+    a.chunk_shift = 32u;
+    if ((chunk & (chunk - 1u)) == 0u)
+        for (uint32_t k = 0; k < 32u; ++k)
+            if ((1u << k) == chunk) a.chunk_shift = k;
     a.counts = reinterpret_cast<uint32_t*>(base);
     a.cursor = reinterpret_cast<uint32_t*>(base + counts_bytes);
     a.offsets = reinterpret_cast<uint32_t*>(base + counts_bytes + align256(4ull * bricks));
