@@ -159,7 +159,7 @@ struct BrickArgs {
     uint32_t bricks;     // per_axis^3
     uint32_t chunk;      // particles per deposit work item
     uint32_t chunk_shift;  // log2(chunk) when chunk is a power of two, else 32
-    uint32_t* counts;    // [kMaxBricks + 1]: counts, then the count pass's finished-block counter; zero between calls
+    uint32_t* counts;    // [kMaxBricks], zero between calls (the scan re-zeroes what it read)
     uint32_t* offsets;   // [bricks + 1], exclusive scan of counts
     uint32_t* cursor;    // [bricks], reservation cursor
     uint32_t* items;     // [bricks + 1], exclusive scan of ceil(count / chunk)
@@ -188,25 +188,27 @@ __device__ __forceinline__ uint32_t brick_items(uint32_t c, const BrickArgs& a) 
 }
 
 // Exclusive scans of the brick counts (offsets, cursor) and of their work
-// items (items), by one block of kBrickBlock threads: each thread scans a
+// items (items), by one block of kScanThreads threads: each thread scans a
 // contiguous run of bricks, loading its counts kScanBatch at a time so the
 // loads are in flight together; the per-thread totals are scanned with warp
-// shuffles and one pass over the warp totals. The counts are read from L2
-// (other blocks added them) and zeroed behind the read, so they start at
-// zero at the next call.
-constexpr uint32_t kScanBatch = 16;
+// shuffles and one pass over the warp totals. The counts are zeroed behind
+// the read, so they start at zero at the next call. (Run by the count
+// kernel's last block instead, the scan's registers cost the count pass its
+// occupancy: 31 -> 56 us at 256^3.)
+constexpr uint32_t kScanBatch = 8;
+constexpr uint32_t kScanThreads = 1024;
 
-__device__ void scan_bricks(const BrickArgs& a) {
-    constexpr uint32_t kWarps = kBrickBlock / 32u;
+__global__ void __launch_bounds__(kScanThreads) brick_scan_kernel(BrickArgs a) {
+    constexpr uint32_t kWarps = kScanThreads / 32u;
     __shared__ uint32_t warp_p[kWarps], warp_i[kWarps];
     const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5;
-    const uint32_t per = (a.bricks + kBrickBlock - 1u) / kBrickBlock;
+    const uint32_t per = (a.bricks + kScanThreads - 1u) / kScanThreads;
     const uint32_t b0 = min(threadIdx.x * per, a.bricks), b1 = min(b0 + per, a.bricks);
     uint32_t sp = 0, si = 0;
     for (uint32_t b = b0; b < b1; b += kScanBatch) {
         uint32_t c[kScanBatch];
 #pragma unroll
-        for (uint32_t j = 0; j < kScanBatch; ++j) c[j] = b + j < b1 ? __ldcg(a.counts + b + j) : 0u;
+        for (uint32_t j = 0; j < kScanBatch; ++j) c[j] = b + j < b1 ? a.counts[b + j] : 0u;
 #pragma unroll
         for (uint32_t j = 0; j < kScanBatch; ++j) {
             sp += c[j];
@@ -233,7 +235,7 @@ __device__ void scan_bricks(const BrickArgs& a) {
     for (uint32_t b = b0; b < b1; b += kScanBatch) {
         uint32_t c[kScanBatch];
 #pragma unroll
-        for (uint32_t j = 0; j < kScanBatch; ++j) c[j] = b + j < b1 ? __ldcg(a.counts + b + j) : 0u;
+        for (uint32_t j = 0; j < kScanBatch; ++j) c[j] = b + j < b1 ? a.counts[b + j] : 0u;
 #pragma unroll
         for (uint32_t j = 0; j < kScanBatch; ++j) {
             if (b + j >= b1) break;
@@ -245,20 +247,16 @@ __device__ void scan_bricks(const BrickArgs& a) {
             oi += brick_items(c[j], a);
         }
     }
-    if (threadIdx.x == kBrickBlock - 1u) {
+    if (threadIdx.x == kScanThreads - 1u) {
         a.offsets[a.bricks] = warp_p[kWarps - 1];
         a.items[a.bricks] = warp_i[kWarps - 1];
-        a.counts[kMaxBricks] = 0u;  // the finished-block counter, for the next call
     }
 }
 
 // Each block histograms its particles' bricks in shared memory and adds the
-// histogram to the counts; the block that finishes last (the counter at
-// counts[kMaxBricks], after a fence, as in a threadfence reduction; nothing
-// waits) then scans them.
+// histogram to the counts.
 __global__ void __launch_bounds__(kBrickBlock) brick_count_kernel(BrickArgs a) {
     extern __shared__ uint32_t hist[];
-    __shared__ bool last;
     for (uint32_t b = threadIdx.x; b < a.bricks; b += blockDim.x) hist[b] = 0u;
     __syncthreads();
     const uint32_t begin = blockIdx.x * kBrickParticlesPerBlock;
@@ -275,13 +273,6 @@ __global__ void __launch_bounds__(kBrickBlock) brick_count_kernel(BrickArgs a) {
     __syncthreads();
     for (uint32_t b = threadIdx.x; b < a.bricks; b += blockDim.x)
         if (hist[b]) atomicAdd(&a.counts[b], hist[b]);
-    __threadfence();
-    __syncthreads();
-    if (threadIdx.x == 0) last = atomicAdd(&a.counts[kMaxBricks], 1u) == gridDim.x - 1u;
-    __syncthreads();
-    if (!last) return;
-    __threadfence();
-    scan_bricks(a);
 }
 
 __global__ void __launch_bounds__(kBrickBlock) brick_scatter_kernel(BrickArgs a) {
@@ -527,10 +518,10 @@ static int splat_bin_shaped(gg_particles* ps, gg_volume* vol, const SplatUniform
     GG_CHECK(check_shape(vol, edge, chunk));
     const uint32_t per = bricks_per_axis(vol->size, edge);
     const uint32_t bricks = per * per * per;
-    // counts (a fixed kMaxBricks + 1 words, whatever the shape, so that the
+    // counts (a fixed kMaxBricks words, whatever the shape, so that the
     // zeros the scan leaves behind stay counts), cursor, offsets, items,
     // sorted slots, keys.
-    const uint64_t counts_bytes = align256(4ull * (kMaxBricks + 1u));
+    const uint64_t counts_bytes = align256(4ull * kMaxBricks);
     const uint64_t words = counts_bytes + align256(4ull * bricks) + align256(4ull * (bricks + 1u)) * 2u;
     const uint64_t bytes = words + 2u * align256(4ull * ps->count);
     const uint64_t capacity_before = vol->brick_scratch_capacity;  // changes when the scratch is reallocated
@@ -568,6 +559,8 @@ static int splat_bin_shaped(gg_particles* ps, gg_volume* vol, const SplatUniform
     vol->brick_counts_zero = false;
     brick_count_kernel<<<blocks, kBrickBlock, hist, ctx->stream>>>(a);
     GG_CHECK(gg::launch_status("brick count"));
+    brick_scan_kernel<<<1, kScanThreads, 0, ctx->stream>>>(a);
+    GG_CHECK(gg::launch_status("brick scan"));
     vol->brick_counts_zero = true;
     brick_scatter_kernel<<<blocks, kBrickBlock, hist, ctx->stream>>>(a);
     GG_CHECK(gg::launch_status("brick scatter"));
