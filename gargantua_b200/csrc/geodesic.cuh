@@ -270,21 +270,12 @@ struct Sample {
     float3 velocity;
 };
 
-// Two trilinear half4 fetches, zero outside the cube (march.metal:15-27).
+// Normalised texture coordinates of a position in the volume cube
+// (march.metal:15-27; the sampler reads zero outside it).
 __device__ __forceinline__ float3 volume_coordinates(float3 p, float half_extent) {
     float inv = 1.0f / (2.0f * half_extent);
     return make_float3((p.x + half_extent) * inv, (p.y + half_extent) * inv, (p.z + half_extent) * inv);
 }
 
-__device__ __forceinline__ Sample sample_volume(float3 p, float half_extent, cudaTextureObject_t em, cudaTextureObject_t vel) {
-    float3 c = volume_coordinates(p, half_extent);
-    float4 e = tex3D<float4>(em, c.x, c.y, c.z);
-    float4 v = tex3D<float4>(vel, c.x, c.y, c.z);
-    Sample s;
-    s.emission = make_float3(e.x, e.y, e.z);
-    s.density = e.w;
-    s.velocity = make_float3(v.x, v.y, v.z);
-    return s;
-}
 
 }  // namespace gg
