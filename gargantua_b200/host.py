@@ -255,6 +255,8 @@ class Context:
         """gg_capture_boundary: t of the capture boundary of the rays
         origin -> base + t axis, bisected in FP64 on the device."""
         o, b, a = (np.ascontiguousarray(v, np.float64) for v in (origin, base, axis))
+        for v, what in ((o, "origin"), (b, "base"), (a, "axis")):
+            expect_size(v, 3, what)
         t = C.c_double()
         check(lib().gg_capture_boundary(self.handle, C.byref(u), ptr(o), ptr(b), ptr(a), lo, hi, rays, rounds,
                                         C.byref(t)))
@@ -349,7 +351,7 @@ class Particles:
 
     def write(self, parts: np.ndarray):
         parts = np.ascontiguousarray(parts, np.float32)
-        assert parts.shape == (self.count, 8)
+        expect_size(parts, self.count * 8, "particle records (count x 8 float32)")
         check(lib().gg_particles_write(self.handle, ptr(parts), self.count))
 
     def checksum(self) -> int:
@@ -450,6 +452,10 @@ class Volume:
         em = np.ascontiguousarray(em, np.uint32)
         mo = np.ascontiguousarray(mo, np.int32)
         ma = np.ascontiguousarray(ma, np.uint32)
+        n3 = self.size ** 3
+        expect_size(em, 2 * n3, "emission sums")
+        expect_size(mo, 3 * n3, "momentum sums")
+        expect_size(ma, n3, "mass sums")
         check(lib().gg_volume_write_sums(self.handle, ptr(em), ptr(mo), ptr(ma)))
 
     def read(self):
@@ -462,6 +468,8 @@ class Volume:
     def write(self, emission: np.ndarray, velocity: np.ndarray):
         e = np.ascontiguousarray(emission, np.float16)
         v = np.ascontiguousarray(velocity, np.float16)
+        expect_size(e, 4 * self.size ** 3, "emission texels (half4)")
+        expect_size(v, 4 * self.size ** 3, "velocity texels (half4)")
         check(lib().gg_volume_write(self.handle, ptr(e), ptr(v)))
 
 
@@ -585,6 +593,8 @@ class Bake:
 
 def write_png(path: str, rgba8: np.ndarray):
     rgba8 = np.ascontiguousarray(rgba8, np.uint8)
+    if rgba8.ndim != 3 or rgba8.shape[2] != 4:
+        raise ValueError(f"a PNG needs height x width x 4 bytes, not shape {rgba8.shape}")
     h, w = rgba8.shape[:2]
     check(lib().gg_write_png(path.encode(), ptr(rgba8), w, h))
 
@@ -604,6 +614,25 @@ class RequestSpec:
     star_seed: int = 1
     flags: int = 0
     volume: "Volume | None" = None  # None: the server's volume
+
+
+def expect_size(a: np.ndarray, values: int, what: str) -> None:
+    """The library reads or writes exactly `values` elements at an array's
+    address: refuse any other size before it does."""
+    if a.size != values:
+        raise ValueError(f"{what}: {a.size} values given, {values} expected")
+
+
+def check_pixel_buffer(output: np.ndarray, pixels: int) -> None:
+    """A request's output array: the library writes pixels x 4 half floats
+    to its address, so anything smaller, strided or of another type is
+    refused here rather than overrun."""
+    if not isinstance(output, np.ndarray) or output.dtype != np.float16:
+        raise TypeError("the output must be a numpy float16 array")
+    if not output.flags["C_CONTIGUOUS"] or not output.flags["WRITEABLE"]:
+        raise ValueError("the output must be a writeable C-contiguous array")
+    if output.size != pixels * 4:
+        raise ValueError(f"the output holds {output.size} half floats; the request writes {pixels * 4}")
 
 
 class Server:
@@ -640,6 +669,7 @@ class Server:
         n = spec.width * spec.height
         if output is None:
             output = np.zeros((n, 4), np.float16)
+        check_pixel_buffer(output, n)
         dbg = np.zeros((n, 4), np.float16) if debug else None
         q = T.Request(spec.azimuth, spec.elevation, spec.distance, spec.fov_y, spec.width, spec.height,
                       spec.step_cap, spec.spin, spec.star_seed & 0xFFFFFFFF, spec.flags,

@@ -65,3 +65,35 @@ def test_exit_codes_and_simple_commands():
     assert r.returncode == 2 and "display" in r.stderr
     r = _run("validate")
     assert r.returncode == 2 and "pytest" in r.stderr
+
+
+def test_request_output_buffers_are_checked_before_the_library_writes():
+    import numpy as np
+    import pytest
+
+    from gargantua_b200.host import check_pixel_buffer
+
+    check_pixel_buffer(np.zeros((6, 4), np.float16), 6)
+    with pytest.raises(ValueError):
+        check_pixel_buffer(np.zeros((5, 4), np.float16), 6)
+    with pytest.raises(TypeError):
+        check_pixel_buffer(np.zeros((6, 4), np.float32), 6)
+    with pytest.raises(ValueError):
+        check_pixel_buffer(np.zeros((6, 8), np.float16)[:, ::2], 6)
+    frozen = np.zeros((6, 4), np.float16)
+    frozen.flags.writeable = False
+    with pytest.raises(ValueError):
+        check_pixel_buffer(frozen, 6)
+
+
+def test_host_writers_refuse_arrays_of_the_wrong_size():
+    import numpy as np
+    import pytest
+
+    from gargantua_b200.host import expect_size, write_png
+
+    expect_size(np.zeros((4, 8)), 32, "records")
+    with pytest.raises(ValueError, match="31 values given, 32 expected"):
+        expect_size(np.zeros(31), 32, "records")
+    with pytest.raises(ValueError):
+        write_png("unused.png", np.zeros((4, 4), np.uint8))
