@@ -141,3 +141,28 @@ def test_library_structs_match_their_ctypes_mirrors(tmp_path):
         assert int(got[cname]) == C.sizeof(struct), cname
         for f in fields:
             assert int(got[f"{cname}.{f}"]) == getattr(struct, f).offset, f"{cname}.{f}"
+
+
+def declared_parameter_counts() -> dict[str, int]:
+    """Each GG_API function's parameter count, from its prototype."""
+    counts = {}
+    for path in sorted(os.listdir(os.path.join(ROOT, "include"))):
+        if not path.endswith(".h"):
+            continue
+        text = re.sub(r"/\*.*?\*/", " ", open(os.path.join(ROOT, "include", path)).read(), flags=re.S)
+        for name, params in re.findall(r"GG_API\s+[^;(]*?\b(gg_\w+)\s*\(([^)]*)\)\s*;", text):
+            params = " ".join(params.split())
+            counts[name] = 0 if params in ("", "void") else params.count(",") + 1
+    return counts
+
+
+def test_python_argument_counts_match_the_prototypes():
+    """A parameter added on one side only would pass garbage through ctypes."""
+    from gargantua_b200 import _lib
+
+    counts = declared_parameter_counts()
+    assert len(counts) == len(set(declared_symbols()))
+    wrong = {n: (len(args), counts[n]) for n, (_, args) in _lib.SIGNATURES.items()
+             if n in counts and len(args) != counts[n]}
+    assert not wrong, wrong
+    assert set(_lib.SIGNATURES) <= set(counts), set(_lib.SIGNATURES) - set(counts)
