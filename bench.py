@@ -61,19 +61,36 @@ FLOPS_SAMPLE = 111              # in-slab gather 67 + static-observer direction 
 SERVE_KERR_TRAFFIC_BYTES = 5835776
 
 
+def stream_length(warmup: int, steps: int, per_step: int, latency_requests: int) -> int:
+    """Requests the run needs: every warm-up and timed slice full, then the
+    open-loop latency replay's requests after them (at least 512)."""
+    return max(STREAM_LENGTH, (warmup + steps) * per_step + latency_requests)
+
+
 def make_stream(seed: int, count: int = STREAM_LENGTH):
-    """The seeded request stream: arrival time and request parameters."""
-    rng = np.random.default_rng(seed)
-    arrivals = np.cumsum(rng.exponential(1.0 / ARRIVAL_RATE, size=count))
+    """The seeded request stream: arrival time and request parameters. The
+    first `n` requests are the same for every count >= n: requests are drawn
+    in blocks of 512 (STREAM_LENGTH), block b from its own generator
+    (seed, b), arrivals continuing from the previous block's last."""
     out = []
-    for k in range(count):
+    for block in range((count + STREAM_LENGTH - 1) // STREAM_LENGTH):
+        out.extend(_stream_block(seed, block, out[-1]["t"] if out else 0.0, len(out)))
+    return out[:count]
+
+
+def _stream_block(seed: int, block: int, t0: float, first: int):
+    rng = np.random.default_rng(seed if block == 0 else [seed, block])
+    arrivals = t0 + np.cumsum(rng.exponential(1.0 / ARRIVAL_RATE, size=STREAM_LENGTH))
+    out = []
+    for j in range(STREAM_LENGTH):
+        k = first + j
         w, h = RESOLUTIONS[rng.integers(len(RESOLUTIONS))]
         cap = STEP_CAPS[rng.integers(len(STEP_CAPS))]
         spin = SPINS[rng.integers(len(SPINS))]
         r = rng.uniform(40.0, 120.0)
         inclination = math.radians(rng.uniform(10.0, 90.0))
         azimuth = rng.uniform(0.0, 2.0 * math.pi)
-        out.append({"t": float(arrivals[k]), "width": w, "height": h, "step_cap": cap, "spin": spin,
+        out.append({"t": float(arrivals[j]), "width": w, "height": h, "step_cap": cap, "spin": spin,
                     "distance": float(r), "elevation": math.pi / 2.0 - inclination, "azimuth": float(azimuth),
                     "seed": seed * 100003 + k})
     return out
@@ -185,6 +202,53 @@ def latency_replay(server, stream):
     return float(np.percentile(lat, 50)), float(np.percentile(lat, 99))
 
 
+# Request classes of the per-class table: every resolution and step budget,
+# Schwarzschild (spin 0) and Kerr (spin 0.5 or 0.9), with the stream's camera
+# distribution. A class serves about CLASS_PIXELS pixels (2 to 32 requests).
+CLASS_PIXELS = 2 * 1920 * 1080
+
+
+def class_requests(width: int, height: int, cap: int, kerr: bool, seed: int):
+    rng = np.random.default_rng(seed)
+    n = int(min(32, max(2, round(CLASS_PIXELS / (width * height)))))
+    out = []
+    for k in range(n):
+        spin = float(rng.choice([0.5, 0.9])) if kerr else 0.0
+        r = rng.uniform(40.0, 120.0)
+        inclination = math.radians(rng.uniform(10.0, 90.0))
+        azimuth = rng.uniform(0.0, 2.0 * math.pi)
+        out.append({"t": 0.0, "width": width, "height": height, "step_cap": cap, "spin": spin, "distance": float(r),
+                    "elevation": math.pi / 2.0 - inclination, "azimuth": float(azimuth), "seed": seed * 1009 + k})
+    return out
+
+
+def class_table(servers: dict) -> list:
+    """Each class served closed-loop by every server in `servers` (name ->
+    Server): ray steps / device span, in G ray-steps/s, and the served
+    server's ratio over each per-request one. Each class is served once
+    untimed first (the servers' pools map the class's target sizes)."""
+    rows = []
+    seed = 500
+    for (w, h) in RESOLUTIONS:
+        for cap in STEP_CAPS:
+            for kerr in (False, True):
+                seed += 1
+                reqs = class_requests(w, h, cap, kerr, seed)
+                pins = pinned_outputs(reqs)
+                row = {"class": f"{w}x{h}/{cap}/{'kerr' if kerr else 'schw'}", "requests": len(reqs)}
+                for name, server in servers.items():
+                    serve_slice(server, reqs, pins)
+                    results, wall, span, _, _ = serve_slice(server, reqs, pins)
+                    steps = sum(r.ray_steps for r in results)
+                    row[name] = round(steps / max(span, 1e-12) / 1e9, 3)
+                    row[name + "_e2e"] = round(steps / max(wall, 1e-12) / 1e9, 3)
+                for name in servers:
+                    if name != "served":
+                        row["x_" + name] = round(row["served"] / max(row[name], 1e-12), 2)
+                rows.append(row)
+    return rows
+
+
 def cpu_sample(slices, seconds: float, threads: int):
     """The oracle's FP64 integrators on a bounded sample of the slices' rays:
     returns (ray steps per second, rays, steps, seconds, description)."""
@@ -281,6 +345,29 @@ def measured_peaks() -> dict:
         return {}
 
 
+def cpu_timed(fn, seconds: float = 1.0) -> float:
+    """Mean seconds of fn() over repeats totalling about `seconds` (at least 1)."""
+    t0 = time.perf_counter()
+    fn()
+    once = time.perf_counter() - t0
+    reps = max(1, min(20, int(seconds / max(once, 1e-6))))
+    t0 = time.perf_counter()
+    for _ in range(reps):
+        fn()
+    return (time.perf_counter() - t0) / reps
+
+
+def cpu_pass_baseline(kind: str, fn_of_threads, units: float, unit: str, sample: str) -> dict:
+    """The FP32 CPU replica of a pass (oracle/replica.c, built with
+    -ffp-contract=off, bit-exact with the kernel) on one host thread and on
+    every host core: `units` of work per call."""
+    cores = os.cpu_count() or 1
+    one = cpu_timed(lambda: fn_of_threads(1))
+    every = cpu_timed(lambda: fn_of_threads(cores))
+    return {"value": units / every, "unit": unit, "cores": cores, "kind": "port",
+            "single_thread": units / one, "sample": sample + f"; FP32 replica, 1 and {cores} threads"}
+
+
 def measure_passes(ctx, g, torch) -> dict:
     """The particle step and the splat, each timed alone with CUDA events on
     the library's stream, L2 flushed before every launch by reading a 256 MB
@@ -322,14 +409,25 @@ def measure_passes(ctx, g, torch) -> dict:
     hbm_src = "MEASURED_PEAKS.json hbm_gbs (measured)" if "hbm_gbs" in peaks else "fallback 6650 GB/s"
     out = {}
 
+    sys.path.insert(0, os.path.join(ROOT, "tests"))
+    import oracle_ffi as O
+
     big = g.Particles(ctx, 4_000_000, seed=1)
     big.advance(10, seed_first=True)
     t = timed(lambda: big.step(1))
     gbs = 64.0 * big.count / t / 1e9
+    su, cdf = big.uniforms(), big.inverse_cdf()
+    cpu_parts = big.read()[:1_000_000].copy()
+
+    def cpu_step(threads):
+        O.step32(cpu_parts, 1, 1, cdf, su.dt, su.alpha, su.temperatureScale, 1, threads)
+
     out["sim"] = {"workload": "4M particles (max preset), one dispatch of 2 substeps", "us": t * 1e6,
                   "value": 2 * big.count / t, "unit": "particle-steps/s",
                   "roofline": {"bound": "hbm", "achieved": gbs, "peak": hbm, "unit": "GB/s", "frac": gbs / hbm,
-                               "bytes_per_launch": 64 * big.count, "peak_source": hbm_src}}
+                               "bytes_per_launch": 64 * big.count, "peak_source": hbm_src},
+                  "cpu_baseline": cpu_pass_baseline("sim", cpu_step, 2.0 * len(cpu_parts), "particle-steps/s",
+                                                    "1M of the 4M particles, one dispatch of 2 substeps")}
     big.close()
 
     ps = g.Particles(ctx, 1_000_000, seed=1)
@@ -354,15 +452,23 @@ def measure_passes(ctx, g, torch) -> dict:
             "shape": {"brick_edge": edge, "chunk": chunk, "chosen_by": "gg_splat_autotune"},
             "roofline": {"bound": "shared atomics" if edge else "global atomics", "achieved": rate, "peak": peak,
                          "unit": "G u32 atomic adds/s", "frac": rate / peak, "peak_source": src,
-                         "global_atomic_peak": atom_peak}}
+                         "global_atomic_peak": atom_peak},
+            "cpu_baseline": cpu_pass_baseline(
+                "splat", lambda threads, ex=exact: O.deposit32(parts, 128, 0, ex, 1, threads=threads), deposits,
+                "deposits/s", "the same 1M particles into 128^3 (sums allocated and zeroed per call)")}
     vol.bin(ps, True)
+    sums = vol.read_sums()
+    bb = ctx.blackbody()[:, :3].copy()
     t = timed(vol.resolve, pre=lambda: vol.bin(ps, True))
     gbs = 64.0 * 128 ** 3 / t / 1e9
     out["splat_resolve"] = {"workload": "128^3 resolve + clear", "us": t * 1e6, "value": 128 ** 3 / t,
                             "unit": "voxels/s",
                             "roofline": {"bound": "hbm", "achieved": gbs, "peak": hbm, "unit": "GB/s",
                                          "frac": gbs / hbm, "bytes_per_launch": 64 * 128 ** 3,
-                                         "peak_source": hbm_src}}
+                                         "peak_source": hbm_src},
+                            "cpu_baseline": cpu_pass_baseline(
+                                "resolve", lambda threads: O.resolve32(*sums, 128, bb, threads=threads), 128 ** 3,
+                                "voxels/s", "the same 128^3 sums (no clear)")}
     vol.close()
     ps.close()
 
@@ -422,6 +528,19 @@ def setup_world(device: int, world: int):
     return ctx, ps, vol
 
 
+def drift_summary(d) -> dict | None:
+    """The 4096-step drift figures that carry the metric's precision bar."""
+    if not d:
+        return None
+    out = {}
+    for kind, label in (("schwarzschild", "E/L"), ("kerr", "Q/null residual")):
+        if kind in d:
+            a, b = d[kind]["fp32_compensated"], d[kind]["fp64_oracle"]
+            out[kind] = {"gauge": label, "p99": a["p99"], "under_1e-5": a["under_1e-5"], "fp64_oracle_p99": b["p99"],
+                         "fp64_oracle_under_1e-5": b["under_1e-5"]}
+    return out
+
+
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
@@ -431,6 +550,7 @@ def main():
     ap.add_argument("--requests-per-step", type=int, default=32)
     ap.add_argument("--latency-requests", type=int, default=48)
     ap.add_argument("--no-plain", action="store_true")
+    ap.add_argument("--no-classes", action="store_true", help="skip the per-class served-vs-per-request table")
     ap.add_argument("--no-passes", action="store_true", help="skip the separate sim and splat timings")
     ap.add_argument("--no-tune", action="store_true", help="serve with the default wave shape")
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
@@ -441,13 +561,14 @@ def main():
     local = int(os.environ.get("LOCAL_RANK", "0"))
     B = args.requests_per_step
     nslices = args.warmup + args.steps
+    count = stream_length(args.warmup, args.steps, B, args.latency_requests)
 
     if args.impl == "reference":
         # The reference's CPU path on rank 0 only; other ranks do no work.
         if rank != 0:
             return
         threads = os.cpu_count() or 1
-        stream = make_stream(1)
+        stream = make_stream(1, count)
         slices = [stream[i * B:(i + 1) * B] for i in range(nslices)]
         budget = max(3.0, args.cpu_seconds / 2)
         for s in slices[:args.warmup]:
@@ -489,8 +610,10 @@ def main():
     ctx, ps, vol = setup_world(local, world)
     peak = ctx.fp32_peak_tflops()
     # Weak scaling: every rank serves its own stream (seed 1 + rank).
-    stream = make_stream(1 + rank)
+    stream = make_stream(1 + rank, count)
     slices = [stream[i * B:(i + 1) * B] for i in range(nslices)]
+    assert all(len(sl) == B for sl in slices), "every slice is full"
+    lat_stream = stream[nslices * B:nslices * B + args.latency_requests]
     shape = {"chunk_rays": 32, "wave_rays": 4 << 20, "max_waves_in_flight": 2, "steps_per_round": 8, "refill_idle": 8,
              "schedule": 0,
              "chosen_by": "defaults"}
@@ -523,7 +646,6 @@ def main():
     steps_total = flops_total = 0.0
     launches = 0
     d2h = 0
-    schw_requests = 0
     drift_over = rays_total = 0
     served_per_step = []
     for s, pin in zip(timed, pins):
@@ -537,7 +659,6 @@ def main():
             steps_total += r.ray_steps
             flops_total += flops_of(q, r)
             d2h += q["width"] * q["height"] * 8
-            schw_requests += 1 if q["spin"] == 0.0 else 0
             rays_total += r.counters.rays
             drift_over += r.counters.overDriftBudget
     barrier()
@@ -566,8 +687,7 @@ def main():
     # The per-request baselines on the same slices: the reference's march as
     # written, and this library's plain FP32 step arithmetic launched per
     # request (what batching and compensation add over it).
-    def plain_baseline(mode):
-        server_plain = g.Server(ctx, vol, mode)
+    def plain_baseline(server_plain):
         serve_slice(server_plain, slices[0], pinned_outputs(slices[0]))
         barrier()
         sampler = ClockSampler(local)
@@ -587,26 +707,32 @@ def main():
         out = {"value": p_steps / p_span, "e2e": p_steps / p_wall, "unit": "ray-steps/s",
                "served_over_plain": value / (p_steps / p_span),
                "served_over_plain_e2e": e2e / (p_steps / p_wall),
-               "per_step_values": per_step, "clocks": p_clocks,
-               "median_step_value": statistics.median(per_step),
+               "per_step": {"min": min(per_step), "median": statistics.median(per_step), "max": max(per_step)},
+               "clocks": p_clocks,
                "served_over_plain_median": statistics.median(served_per_step) / statistics.median(per_step)}
-        lat = stream[nslices * B:nslices * B + args.latency_requests]
-        if len(lat) >= 8:
-            out["p50_ms"], out["p99_ms"] = latency_replay(server_plain, lat)
-        server_plain.close()
+        if len(lat_stream) >= 8:
+            out["p50_ms"], out["p99_ms"] = latency_replay(server_plain, lat_stream)
         return out
 
     plain = plain_lane = None
+    plain_servers = {}
     if not args.no_plain:
-        plain = plain_baseline(g.types.SERVE_SERIAL_PLAIN_AS_WRITTEN)
+        plain_servers = {"as_written": g.Server(ctx, vol, g.types.SERVE_SERIAL_PLAIN_AS_WRITTEN),
+                         "plain": g.Server(ctx, vol, g.types.SERVE_SERIAL_PLAIN)}
+        plain = plain_baseline(plain_servers["as_written"])
         plain["kernel"] = "per-request image kernel, the reference's step arithmetic as written (march.metal)"
-        plain_lane = plain_baseline(g.types.SERVE_SERIAL_PLAIN)
+        plain_lane = plain_baseline(plain_servers["plain"])
         plain_lane["kernel"] = "per-request image kernel, this library's plain FP32 step arithmetic"
 
-    lat_stream = stream[nslices * B:nslices * B + args.latency_requests]
     p50 = p99 = None
     if len(lat_stream) >= 8:
         p50, p99 = latency_replay(batched, lat_stream)
+
+    classes = None
+    if not args.no_classes and plain_servers:
+        classes = class_table({"served": batched, **plain_servers})
+    for server in plain_servers.values():
+        server.close()
 
     passes = measure_passes(ctx, g, torch) if not args.no_passes else None
 
@@ -619,6 +745,17 @@ def main():
         cpu = {"value": cv, "unit": "ray-steps/s", "cores": threads, "kind": "port", "sample": desc}
 
     achieved = flops_total / busy / 1e12
+    summary = {
+        "served_G_ray_steps_s": round(value / 1e9, 2),
+        "served_over_plain_as_written": round(plain["served_over_plain"], 3) if plain else None,
+        "served_over_plain_lane": round(plain_lane["served_over_plain"], 3) if plain_lane else None,
+        "p50_ms": p50, "p99_ms": p99,
+        "plain_as_written_p50_p99_ms": [plain.get("p50_ms"), plain.get("p99_ms")] if plain else None,
+        "timed_requests": len(timed) * B, "latency_requests": len(lat_stream),
+        "drift_4096": drift_summary(drift_oracle),
+        "classes_x_as_written_x_plain": ({r["class"]: [r.get("x_as_written"), r.get("x_plain")] for r in classes}
+                                         if classes else None),
+    }
     line = {
         "metric": "ray-steps/s, served mixed request stream (4096-step E/L drift < 1e-5), p50/p99 ms",
         "value": value,
@@ -634,14 +771,17 @@ def main():
         "data": "synthetic",
         "config": {"workload": "served mixed request stream (configs: 40 req/s Poisson; 320x180..3840x2160; "
                                "256/4096 steps; spin 0/0.5/0.9; r 40-120; 1M-particle settled disk, 128^3)",
-                   "requests_per_step": B, "stream_seed": 1, "precision": "compensated FP32 + FP64 re-integration",
+                   "requests_per_step": B, "stream_seed": 1, "stream_requests": count,
+                   "precision": "compensated FP32 + FP64 re-integration",
                    "server_shape": shape,
                    "l2": "inputs larger than L2 (outputs up to 66 MB per request, 8-200 MB per step)"},
         "p50_ms": p50,
         "p99_ms": p99,
-        "per_step_values": served_per_step,
+        "per_step": {"min": min(served_per_step), "median": statistics.median(served_per_step),
+                     "max": max(served_per_step)},
         "plain_per_request": plain,
         "plain_lane_per_request": plain_lane,
+        "classes": classes,
         "drift": {"rays": rays_total, "over_budget": drift_over, "vs_fp64_oracle": drift_oracle},
         "e2e": {"value": e2e, "unit": "ray-steps/s", "h2d_bytes_per_step": int(B * 64),
                 "d2h_bytes_per_step": int(d2h / max(args.steps, 1))},
@@ -656,7 +796,9 @@ def main():
         "cpu_baseline": cpu,
         "passes": passes,
         "clocks": clock_info,
-        "gpu_launches": int(launches * 2 + schw_requests * 2),
+        # Kernels the server launched in the timed steps (gg_server_totals).
+        "gpu_launches": int(sum_over_ranks(launches)),
+        "summary": summary,
     }
     batched.close()
     if dist is not None:

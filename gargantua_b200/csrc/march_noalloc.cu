@@ -14,10 +14,15 @@
 // The scratch is one file-scope __device__ array of NOALLOC_MAX_PIXELS + 64
 // words (about 8 MiB); every GPU that loads the library holds it until the
 // process exits. Host code cannot pass the array's name to a kernel (on the
-// host it names a host-side stand-in, not device memory), so the first call
-// on each device, with that device current, asks the runtime for the
-// array's device address with cudaGetSymbolAddress and keeps it; make that
-// first call before any stream capture. Every call on a device shares the
+// host it names a host-side stand-in, not device memory), so each call, with
+// its device current, asks the runtime for the array's device address with
+// cudaGetSymbolAddress. The first such lookup on a device loads the array
+// (set-up); make that first call before any stream capture. While the
+// context's stream is being captured the address recorded by the last
+// uncaptured call on that device is used instead, so a capture never does
+// the set-up; looking the address up again on the other calls keeps it
+// right after a cudaDeviceReset, which may place the array elsewhere.
+// Every call on a device shares the
 // array and reuses what the last call left in it: each call zeroes the list
 // counter on its stream before the march, and two calls whose work overlaps
 // on the GPU (different streams or contexts on one device) race on the
@@ -44,16 +49,24 @@ constexpr int kMaxDevices = 64;
 static std::mutex g_noalloc_mu;
 static uint32_t* g_noalloc_address[kMaxDevices] = {};
 
-// The array's device address on `device` (current), looked up once.
-static int noalloc_scratch(int device, uint32_t** out) {
+// The array's device address on `device` (current). Looked up on every call
+// made outside a stream capture; a call made while `stream` is capturing
+// reuses the address the last uncaptured call on the device recorded.
+static int noalloc_scratch(int device, cudaStream_t stream, uint32_t** out) {
     if (device < 0 || device >= kMaxDevices)
         return fail(GG_ERR_UNSUPPORTED, "Device %d is beyond the %d devices the fixed scratch tracks.", device, kMaxDevices);
+    cudaStreamCaptureStatus capture = cudaStreamCaptureStatusNone;
+    GG_CUDA(cudaStreamIsCapturing(stream, &capture), "fixed scratch: capture status");
     std::lock_guard<std::mutex> lock(g_noalloc_mu);
-    if (!g_noalloc_address[device]) {
+    if (capture == cudaStreamCaptureStatusNone) {
         void* p = nullptr;
         cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
         if (e != cudaSuccess) return cuda_status(e, "fixed scratch address");
         g_noalloc_address[device] = static_cast<uint32_t*>(p);
+    } else if (!g_noalloc_address[device]) {
+        return fail(GG_ERR_UNSUPPORTED,
+                    "gg_march_compensated_noalloc: the first call on device %d must come before any stream capture.",
+                    device);
     }
     *out = g_noalloc_address[device];
     return GG_OK;
@@ -74,7 +87,7 @@ extern "C" GG_API int gg_march_compensated_noalloc(gg_context* ctx, const gg_vol
                         "gg_march_compensated_noalloc serves targets of at most %u pixels; %ux%u is %llu.",
                         gg::kNoAllocMaxPixels, targets->width, targets->height, (unsigned long long)pixels);
     uint32_t* scratch = nullptr;
-    GG_CHECK(gg::noalloc_scratch(ctx->device, &scratch));
+    GG_CHECK(gg::noalloc_scratch(ctx->device, ctx->stream, &scratch));
     gg::MarchParams p = gg::make_params(ctx, vol, *u, &ctx->sweep);
     p.color = targets->color;
     p.debug = targets->debug;

@@ -448,7 +448,10 @@ struct gg_server {
     std::string fatal_sentence;
     int injected = GG_OK;  // gg_server_inject_fault: the next device call "fails" with this status
     std::thread worker;
-    uint64_t total_requests = 0, total_steps = 0, total_waves = 0;
+    // total_launches: kernels launched (each wave's two persistent kernels and
+    // its FP64 pass, each Schwarzschild request's two sweep-table builds, one
+    // image kernel per request in the plain modes).
+    uint64_t total_requests = 0, total_steps = 0, total_launches = 0;
     std::vector<std::pair<double, double>> intervals;  // wave device intervals, seconds after `origin`
     int next_slot = 0;
 };
@@ -508,6 +511,7 @@ static int admit(gg_server* s, const std::shared_ptr<ServedRequest>& r) {
                 "sky table");
         GG_CHECK(sweep_build(ctx, s->build, (double)r->q.distance, &r->sweep));
         sweep_apply(ctx, &r->sweep, &r->u);
+        s->total_launches += 2;
     }
     r->result.admitted = now_seconds();
     return GG_OK;
@@ -622,7 +626,7 @@ static int launch_wave(gg_server* s, WaveSlot& w) {
     GG_CHECK(launch_status("FP64 re-integration"));
     GG_CUDA(cudaEventRecord(w.fp64_done, w.fp64), "wave event");
     w.busy = true;
-    s->total_waves += 1;
+    s->total_launches += 3;
     return GG_OK;
 }
 
@@ -645,7 +649,10 @@ static int finish_wave(gg_server* s, WaveSlot& w) {
 }
 
 // The per-request baseline: one request at a time, plain FP32 image kernel.
-static int run_plain(gg_server* s, ServedRequest& r) {
+// Runs with the server's mutex released, so it touches no shared server
+// state: the launch's device interval is returned in *interval and the
+// caller records it (and the launch count) once it holds the mutex again.
+static int run_plain(gg_server* s, ServedRequest& r, std::pair<double, double>* interval) {
     gg_context* ctx = s->ctx;
     GG_CUDA(cudaStreamWaitEvent(s->plain, s->built, 0), "plain ordering");
     MarchParams p = make_params(ctx, request_volume(s, r), r.u, r.q.spin == 0.0f ? &r.sweep : nullptr);
@@ -659,14 +666,13 @@ static int run_plain(gg_server* s, ServedRequest& r) {
     GG_CHECK(launch_plain_image(p, s->plain, s->cfg.mode == GG_SERVE_SERIAL_PLAIN_AS_WRITTEN));
     GG_CUDA(cudaEventRecord(s->slots[0].stop, s->plain), "plain event");
     r.next_ray = r.rays;
-    s->total_waves += 1;
     GG_CHECK(start_copy(s, r, s->slots[0].stop));
     // Serial: the next request starts after this one's pixels are home.
     GG_CUDA(cudaEventSynchronize(r.copied), "plain march");
     float t0 = 0.0f, t1 = 0.0f;
     GG_CUDA(cudaEventElapsedTime(&t0, s->origin, s->slots[0].start), "plain timing");
     GG_CUDA(cudaEventElapsedTime(&t1, s->origin, s->slots[0].stop), "plain timing");
-    s->intervals.emplace_back((double)t0 * 1e-3, (double)t1 * 1e-3);
+    *interval = std::make_pair((double)t0 * 1e-3, (double)t1 * 1e-3);
     return GG_OK;
 }
 
@@ -718,9 +724,14 @@ static void worker_loop(gg_server* s) {
             if (serial(s)) {
                 for (auto& r : s->admitted)
                     if (r->next_ray < r->rays && status == GG_OK) {
+                        std::pair<double, double> interval(0.0, 0.0);
                         lock.unlock();
-                        status = run_plain(s, *r);
+                        status = run_plain(s, *r, &interval);
                         lock.lock();
+                        if (status == GG_OK) {
+                            s->total_launches += 1;
+                            s->intervals.push_back(interval);
+                        }
                     }
             } else {
                 for (uint32_t k = 0; k < s->slots.size() && status == GG_OK; ++k) {
@@ -1018,7 +1029,7 @@ GG_API int gg_server_totals(gg_server* s, int reset, uint64_t* requests, uint64_
     std::lock_guard<std::mutex> lock(s->mu);
     if (requests) *requests = s->total_requests;
     if (ray_steps) *ray_steps = s->total_steps;
-    if (launches) *launches = s->total_waves;
+    if (launches) *launches = s->total_launches;
     // Union of the launch intervals: waves on different streams overlap.
     std::vector<std::pair<double, double>> iv = s->intervals;
     std::sort(iv.begin(), iv.end());
@@ -1033,7 +1044,7 @@ GG_API int gg_server_totals(gg_server* s, int reset, uint64_t* requests, uint64_
     if (busy_seconds) *busy_seconds = busy;
     if (span_seconds) *span_seconds = iv.empty() ? 0.0 : last - first;
     if (reset) {
-        s->total_requests = s->total_steps = s->total_waves = 0;
+        s->total_requests = s->total_steps = s->total_launches = 0;
         s->intervals.clear();
     }
     return GG_OK;

@@ -332,8 +332,10 @@ GG_API int gg_capture_boundary(gg_context* ctx, const MarchUniforms* u, const do
  * every GPU loading the library holds until exit, and targets larger than
  * NOALLOC_MAX_PIXELS are refused with GG_ERR_INVALID_ARGUMENT. The caller
  * passes inputs and outputs as for gg_march (sweep tables, when enabled,
- * come from an earlier gg_tables_update). The first call on each device
- * looks up the array's device address; make it before any stream capture.
+ * come from an earlier gg_tables_update). Each call looks up the array's
+ * device address (the first lookup on a device loads the array: make that
+ * first call before any stream capture; a call during a capture of the
+ * context's stream reuses the last address looked up on the device).
  * All calls on a device share the array: calls whose work overlaps on the
  * GPU race, so serialise them. This entry point has no counterpart in the
  * reference, whose host allocates every buffer up front. */
@@ -482,7 +484,9 @@ GG_API int gg_server_poll(gg_server* s, uint64_t ticket, int* done);
 GG_API int gg_server_wait(gg_server* s, uint64_t ticket, double timeout_s, gg_request_result* result);
 
 /* Totals since creation or the last reset: requests completed, ray steps,
- * launches (waves, or per-request kernels in the plain mode), device-busy
+ * kernel launches (each wave's two persistent kernels and its FP64 pass,
+ * each Schwarzschild request's two sweep-table builds, or one image kernel
+ * per request in the plain modes), device-busy
  * seconds (union of the launches' CUDA-event intervals) and device span
  * seconds (first launch start to last launch end, on the device clock).
  * reset != 0 zeroes them after reading. Any output pointer may be NULL. */

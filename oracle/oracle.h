@@ -174,13 +174,13 @@ uint64_t o_fnv1a(const void* bytes, uint64_t count);
  * layouts: emission u32[2 n^3], momentum i32[3 n^3], mass u32[n^3]. */
 void o32_deposit(const float* particles, uint32_t count, uint32_t size, float half_extent, float peak_temperature,
                  float emission_scale, uint32_t frame, uint32_t exact, uint32_t seed_lo, uint32_t seed_hi,
-                 uint32_t* emission, int32_t* momentum, uint32_t* mass, uint32_t first_index);
+                 uint32_t* emission, int32_t* momentum, uint32_t* mass, uint32_t first_index, int threads);
 
 /* Resolve (splat.metal:93-120) in FP32 with a float blackbody table
  * (count x 3, linearly interpolated); outputs float rgba per voxel. */
 void o32_resolve(const uint32_t* emission, const int32_t* momentum, const uint32_t* mass, uint32_t size,
                  float half_extent, float peak_temperature, const float* blackbody_rgb, int bb_count,
-                 float* emission_out, float* velocity_out);
+                 float* emission_out, float* velocity_out, int threads);
 
 /* PBR Neutral (present.metal:22-35) on one colour. */
 void o_pbr_neutral(const double in[3], double out[3]);

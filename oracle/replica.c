@@ -180,28 +180,49 @@ uint64_t o_fnv1a(const void* bytes, uint64_t count) {
     return hash;
 }
 
+/* Add v to *word; shared between threads when `atomic` (the sums are
+ * integers, so the order of the adds does not change the result). */
+static inline void add_u32(uint32_t* word, uint32_t v, int atomic) {
+    if (atomic) {
+#pragma omp atomic
+        *word += v;
+    } else {
+        *word += v;
+    }
+}
+
 /* splat.metal:25-37: one corner's six fixed-point sums */
 static void deposit32(uint32_t* em, int32_t* mo, uint32_t* ma, uint32_t index, float weight, float energy,
-                      float relative, float vx, float vy, float vz) {
+                      float relative, float vx, float vy, float vz, int atomic) {
     uint32_t fe = (uint32_t)(energy * weight * 16777216.0f + 0.5f);
     uint32_t fet = (uint32_t)(energy * relative * weight * 1048576.0f + 0.5f);
     float ms = weight * 4096.0f;
     int32_t mx = (int32_t)rintf(vx * ms), my = (int32_t)rintf(vy * ms), mz = (int32_t)rintf(vz * ms);
     uint32_t fm = (uint32_t)(weight * 256.0f + 0.5f);
-    em[2u * index + 0u] += fe;
-    em[2u * index + 1u] += fet;
-    /* two's complement wraparound, as the device's integer atomics */
-    mo[3u * index + 0u] = (int32_t)((uint32_t)mo[3u * index + 0u] + (uint32_t)mx);
-    mo[3u * index + 1u] = (int32_t)((uint32_t)mo[3u * index + 1u] + (uint32_t)my);
-    mo[3u * index + 2u] = (int32_t)((uint32_t)mo[3u * index + 2u] + (uint32_t)mz);
-    ma[index] += fm;
+    /* momentum words add in two's complement with wraparound, as the
+     * device's integer atomics do */
+    uint32_t* mu = (uint32_t*)mo;
+    add_u32(&em[2u * index + 0u], fe, atomic);
+    add_u32(&em[2u * index + 1u], fet, atomic);
+    add_u32(&mu[3u * index + 0u], (uint32_t)mx, atomic);
+    add_u32(&mu[3u * index + 1u], (uint32_t)my, atomic);
+    add_u32(&mu[3u * index + 2u], (uint32_t)mz, atomic);
+    add_u32(&ma[index], fm, atomic);
 }
 
-/* splat.metal:44-88 */
+/* splat.metal:44-88. threads == 1 deposits serially; otherwise the particles
+ * are split over OpenMP threads (threads <= 0: the runtime's default count)
+ * that add into the shared sums atomically. */
 void o32_deposit(const float* particles, uint32_t count, uint32_t n, float half_extent, float peak_temperature,
                  float emission_scale, uint32_t frame, uint32_t exact, uint32_t seed_lo, uint32_t seed_hi,
-                 uint32_t* em, int32_t* mo, uint32_t* ma, uint32_t first_index) {
-    for (uint32_t i = 0; i < count; ++i) {
+                 uint32_t* em, int32_t* mo, uint32_t* ma, uint32_t first_index, int threads) {
+    const int atomic = threads != 1;
+#ifdef _OPENMP
+    if (threads > 1) omp_set_num_threads(threads);
+#endif
+#pragma omp parallel for schedule(static) if (atomic)
+    for (int64_t ii = 0; ii < (int64_t)count; ++ii) {
+        const uint32_t i = (uint32_t)ii;
         const float* p = particles + 8 * (uint64_t)i;
         float pos[3] = {p[0], p[1], p[2]};
         float unit[3];
@@ -235,7 +256,7 @@ void o32_deposit(const float* particles, uint32_t count, uint32_t n, float half_
                 float w = w3[0] * w3[1] * w3[2];
                 if (w <= 0.0f) continue;
                 uint32_t index = ((uint32_t)corner[2] * n + (uint32_t)corner[1]) * n + (uint32_t)corner[0];
-                deposit32(em, mo, ma, index, w, energy, relative, p[3], p[4], p[5]);
+                deposit32(em, mo, ma, index, w, energy, relative, p[3], p[4], p[5], atomic);
             }
         } else {
             uint32_t h[4];
@@ -243,7 +264,7 @@ void o32_deposit(const float* particles, uint32_t count, uint32_t n, float half_
             int corner[3];
             for (int a = 0; a < 3; ++a) corner[a] = unitf(h[a]) < frac[a] ? high[a] : low[a];
             uint32_t index = ((uint32_t)corner[2] * n + (uint32_t)corner[1]) * n + (uint32_t)corner[0];
-            deposit32(em, mo, ma, index, 1.0f, energy, relative, p[3], p[4], p[5]);
+            deposit32(em, mo, ma, index, 1.0f, energy, relative, p[3], p[4], p[5], atomic);
         }
     }
 }
@@ -257,13 +278,19 @@ static float bb_coordinate(float temperature) {
     return (float)((gg_log_d((double)t) - lo) / (hi - lo));
 }
 
-/* splat.metal:93-120 with the linear clamp-to-edge lookup done in FP32 */
+/* splat.metal:93-120 with the linear clamp-to-edge lookup done in FP32.
+ * Voxels are split over `threads` OpenMP threads (1: serial; <= 0: the
+ * runtime's default count); each voxel is independent. */
 void o32_resolve(const uint32_t* em, const int32_t* mo, const uint32_t* ma, uint32_t n, float half_extent,
-                 float peak_temperature, const float* bb, int bb_count, float* eo, float* vo) {
+                 float peak_temperature, const float* bb, int bb_count, float* eo, float* vo, int threads) {
     float voxel = 2.0f * half_extent / (float)n;
     float inverse_volume = 1.0f / (voxel * voxel * voxel);
-    uint64_t total = (uint64_t)n * n * n;
-    for (uint64_t index = 0; index < total; ++index) {
+    int64_t total = (int64_t)n * n * n;
+#ifdef _OPENMP
+    if (threads > 1) omp_set_num_threads(threads);
+#endif
+#pragma omp parallel for schedule(static) if (threads != 1)
+    for (int64_t index = 0; index < total; ++index) {
         float count = (float)ma[index] / 256.0f;
         float energy = (float)em[2 * index + 0] / 16777216.0f;
         float energy_t = (float)em[2 * index + 1] / 1048576.0f;

@@ -11,7 +11,7 @@ data is carried over as files:
                       symbol -> numeric value, so a CPU test can check that
                       include/gargantua_constants.h carries the same numbers
 
-Usage: python tests/golden/make_fixtures.py [/path/to/reference]
+Usage: python tests/golden/make_fixtures.py /path/to/gargantua
 """
 import json
 import os
@@ -46,4 +46,6 @@ def main(reference: str) -> None:
 
 
 if __name__ == "__main__":
-    main(sys.argv[1] if len(sys.argv) > 1 else "/root/reference")
+    if len(sys.argv) != 2:
+        sys.exit("usage: make_fixtures.py /path/to/gargantua (the reference's source tree)")
+    main(sys.argv[1])

@@ -155,8 +155,8 @@ def lib() -> C.CDLL:
         "o32_seed_profile": (None, [_fp, u32, u32, u32, u32, _fp, u32, C.c_float, u32, _fp, C.c_float]),
         "o_fnv1a": (u64, [C.c_void_p, u64]),
         "o32_deposit": (None, [_fp, u32, u32, C.c_float, C.c_float, C.c_float, u32, u32, u32, u32, _u32p, _i32p, _u32p,
-                                u32]),
-        "o32_resolve": (None, [_u32p, _i32p, _u32p, u32, C.c_float, C.c_float, _fp, i, _fp, _fp]),
+                                u32, i]),
+        "o32_resolve": (None, [_u32p, _i32p, _u32p, u32, C.c_float, C.c_float, _fp, i, _fp, _fp, i]),
         "o_pbr_neutral": (None, [_dp, _dp]),
     }
     for name, (res, args) in sig.items():
@@ -293,23 +293,25 @@ def fnv1a(buf: np.ndarray) -> int:
 
 
 def deposit32(parts: np.ndarray, size: int, frame: int, exact: bool, seed: int, half_extent: float = 30.0,
-              peak_temperature: float = 8000.0, emission_scale: float = 5e-4, first_index: int = 0):
+              peak_temperature: float = 8000.0, emission_scale: float = 5e-4, first_index: int = 0,
+              threads: int = 1):
     n3 = size ** 3
     em = np.zeros(2 * n3, np.uint32)
     mo = np.zeros(3 * n3, np.int32)
     ma = np.zeros(n3, np.uint32)
     lib().o32_deposit(np.ascontiguousarray(parts, np.float32), len(parts), size, half_extent, peak_temperature,
                       emission_scale, frame, 1 if exact else 0, seed & 0xFFFFFFFF, seed >> 32, em, mo, ma,
-                      first_index)
+                      first_index, threads)
     return em, mo, ma
 
 
-def resolve32(em, mo, ma, size: int, bb_rgb: np.ndarray, half_extent: float = 30.0, peak_temperature: float = 8000.0):
+def resolve32(em, mo, ma, size: int, bb_rgb: np.ndarray, half_extent: float = 30.0, peak_temperature: float = 8000.0,
+              threads: int = 1):
     n3 = size ** 3
     eo = np.zeros((n3, 4), np.float32)
     vo = np.zeros((n3, 4), np.float32)
     bb = np.ascontiguousarray(bb_rgb, np.float32)
-    lib().o32_resolve(em, mo, ma, size, half_extent, peak_temperature, bb, len(bb), eo, vo)
+    lib().o32_resolve(em, mo, ma, size, half_extent, peak_temperature, bb, len(bb), eo, vo, threads)
     return eo, vo
 
 

@@ -44,3 +44,27 @@ def test_arrivals_are_poisson_at_forty_per_second():
     assert 34.0 < rate < 46.0  # 512 exponential gaps: the sample rate is within ~12 %
     # exponential gaps: the coefficient of variation is near 1
     assert 0.8 < gaps.std() / gaps.mean() < 1.2
+
+
+def test_every_slice_and_the_latency_replay_are_full_at_any_step_count():
+    """bench.py --steps 20 --warmup 5 at 32 requests per step needs 800 timed
+    and warm-up requests plus 48 for the open-loop latency replay; the stream
+    grows to cover them, and its first 512 requests do not change."""
+    for warmup, steps, per_step, latency in [(5, 20, 32, 48), (3, 8, 32, 48), (1, 1, 2, 0)]:
+        count = bench.stream_length(warmup, steps, per_step, latency)
+        s = bench.make_stream(1, count)
+        slices = [s[i * per_step:(i + 1) * per_step] for i in range(warmup + steps)]
+        assert all(len(sl) == per_step for sl in slices)
+        assert len(s[(warmup + steps) * per_step:(warmup + steps) * per_step + latency]) == latency
+    assert bench.make_stream(1, 900)[:512] == bench.make_stream(1)
+
+
+def test_class_requests_cover_one_class_each():
+    for (w, h) in bench.RESOLUTIONS:
+        for cap in bench.STEP_CAPS:
+            for kerr in (False, True):
+                reqs = bench.class_requests(w, h, cap, kerr, 7)
+                assert 2 <= len(reqs) <= 32
+                assert {(q["width"], q["height"], q["step_cap"]) for q in reqs} == {(w, h, cap)}
+                spins = {q["spin"] for q in reqs}
+                assert spins <= ({0.5, 0.9} if kerr else {0.0})

@@ -75,6 +75,44 @@ def test_noalloc_matches_gg_march_on_two_calls(scene, spin, step_cap):
     ref_t.close()
 
 
+def test_noalloc_reintegrates_the_same_rays_and_allocates_nothing(scene):
+    """A Kerr still close to the hole (a = 0.9, camera at r = 9, 4096 steps,
+    every flagged ray re-integrated) puts rays on the FP64 list, so the fixed
+    array is written and read: the FP64 ray count and the pixels must equal
+    gg_march's on two calls in a row, and the device's free memory must not
+    move across the calls after the first (which loads the array)."""
+    import torch
+
+    import gargantua_b200 as g
+
+    ctx, vol = scene
+    cam = g.OrbitCamera(0.4, 0.3, 9.0)
+    st = g.Settings.still()
+    u = g.uniforms(cam, 256, 144, st, 1e-5, True, 5, spin=0.9)
+    ctx.set_fp64_policy(g.types.FP64_ALL_FLAGGED)
+    try:
+        ref_t = g.Targets(ctx, 256, 144)
+        g.march(ctx, vol, u, ref_t, g.types.PRECISION_COMPENSATED)
+        ref_fp64 = g.march_stats(ctx)[2]
+        ref_color, _, _ = ref_t.read()
+        assert ref_fp64 > 0
+        t = g.Targets(ctx, 256, 144)
+        free = []
+        for call in range(3):
+            status, _ = noalloc(ctx, vol, u, t)
+            assert status == 0, g.lib().gg_last_error()
+            ctx.synchronize()
+            free.append(torch.cuda.mem_get_info(0)[0])
+            assert g.march_stats(ctx)[2] == ref_fp64, call
+            color, _, _ = t.read()
+            assert np.array_equal(color.view(np.uint16), ref_color.view(np.uint16)), call
+        assert free[1] == free[0] and free[2] == free[0], free
+        t.close()
+        ref_t.close()
+    finally:
+        ctx.set_fp64_policy(g.types.FP64_ESCAPING)
+
+
 def test_noalloc_refuses_targets_beyond_its_scratch(scene):
     import gargantua_b200 as g
 
