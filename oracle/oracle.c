@@ -30,6 +30,7 @@ static const double PI = 3.14159265358979323846;
 #define C_CEILING 0.85
 #define C_BEAM_FLOOR 40.0
 #define C_KERR_MARGIN 0.05
+#define C_BCRIT 5.196152422706632
 
 static double dmin(double a, double b) { return a < b ? a : b; }
 static double dmax(double a, double b) { return a > b ? a : b; }
@@ -471,6 +472,69 @@ void o_integrate_batch(const double* probes, int n, const o_settings* st, double
         out[8] = (double)steps;
         out[9] = ray.energy;
         out[10] = ray.angular_momentum;
+    }
+}
+
+/* ------------------------------------------------------------ bake.metal */
+
+/* bakeRays (bake.metal:46-91) in FP64 for rays launched at the camera (no
+ * sphere jump): integrate with the oracle's step and step policy; after each
+ * step, a point inside the disk slab (|z| < 6, |x|, |y| < half_extent) at
+ * least `spacing` of path since the last stored one is stored (position and
+ * that path), up to `capacity` points (a ray with more is `overflowed`).
+ * Per ray: samples[capacity][4], count, overflowed, falls_in (captured, or
+ * exhausted inbound inside the critical impact parameter), final direction
+ * and depth (path to the first stored point, else the whole path, over
+ * 2 R_ESCAPE, at most 1). */
+void o_bake_batch(const double* probes, int n, const o_settings* st, double spacing, double half_extent, int capacity,
+                  double* samples, int* counts, int* overflowed, int* falls_in, double* direction_depth, int threads) {
+#ifdef _OPENMP
+    if (threads > 0) omp_set_num_threads(threads);
+#endif
+#pragma omp parallel for schedule(dynamic, 1)
+    for (int i = 0; i < n; ++i) {
+        o_ray ray;
+        o_launch(probes + 6 * i, probes + 6 * i + 3, &ray);
+        double* slot = samples + (int64_t)i * capacity * 4;
+        double previous[3];
+        o_ray_position(&ray, previous);
+        double since = 0.0, travelled = 0.0, first_depth = -1.0;
+        int count = 0, over = 0, outcome = O_EXHAUSTED;
+        for (int64_t k = 0; k < st->step_cap; ++k) {
+            double h = o_step_length(st, ray.s[1], previous[2]);
+            double next[6];
+            o_step(ray.s, h, next);
+            memcpy(ray.s, next, sizeof next);
+            double pos[3];
+            o_ray_position(&ray, pos);
+            double d[3] = {pos[0] - previous[0], pos[1] - previous[1], pos[2] - previous[2]};
+            double path = sqrt(dot3(d, d));
+            since += path;
+            travelled += path;
+            memcpy(previous, pos, sizeof pos);
+            if (ray.s[1] <= st->capture_radius) { outcome = O_CAPTURED; break; }
+            if (fabs(pos[2]) < C_SLAB && fabs(pos[0]) < half_extent && fabs(pos[1]) < half_extent && since >= spacing) {
+                if (count < capacity) {
+                    slot[4 * count + 0] = pos[0];
+                    slot[4 * count + 1] = pos[1];
+                    slot[4 * count + 2] = pos[2];
+                    slot[4 * count + 3] = since;
+                    count += 1;
+                    if (first_depth < 0.0) first_depth = travelled;
+                } else {
+                    over = 1;
+                }
+                since = 0.0;
+            }
+            if (ray.s[1] >= st->escape_radius) { outcome = O_ESCAPED; break; }
+        }
+        counts[i] = count;
+        overflowed[i] = over;
+        falls_in[i] = outcome == O_CAPTURED ||
+                      (outcome == O_EXHAUSTED && ray.s[4] < 0.0 && fabs(ray.angular_momentum) < C_BCRIT * ray.energy);
+        o_ray_direction(&ray, direction_depth + 4 * i);
+        double depth = first_depth >= 0.0 ? first_depth : travelled;
+        direction_depth[4 * i + 3] = dmin(depth / (2.0 * C_ESCAPE), 1.0);
     }
 }
 

@@ -103,6 +103,12 @@ double o_critical_impact_parameter(double launch_radius, const o_settings* st, i
  * position xyz, direction xyz, drift, outcome, steps, energy, L. */
 void o_integrate_batch(const double* probes, int n, const o_settings* st, double* results, int threads);
 
+/* bakeRays (bake.metal:46-91) in FP64 for rays launched at the camera (no
+ * sphere jump). samples: n x capacity x (x, y, z, path since the previous
+ * stored point); direction_depth: n x (final direction xyz, depth). */
+void o_bake_batch(const double* probes, int n, const o_settings* st, double spacing, double half_extent, int capacity,
+                  double* samples, int* counts, int* overflowed, int* falls_in, double* direction_depth, int threads);
+
 /* KerrGeodesic.swift:9-281. state: r theta phi pr ptheta energy L */
 typedef struct { double step_factor, step_min, step_max, capture_margin, escape_radius; int64_t step_cap; } o_kerr_settings;
 void o_kerr_settings_default(o_kerr_settings* s, int64_t step_cap);
@@ -181,6 +187,18 @@ void o32_deposit(const float* particles, uint32_t count, uint32_t size, float ha
 void o32_resolve(const uint32_t* emission, const int32_t* momentum, const uint32_t* mass, uint32_t size,
                  float half_extent, float peak_temperature, const float* blackbody_rgb, int bb_count,
                  float* emission_out, float* velocity_out, int threads);
+
+/* The tone-map kernel's arithmetic in FP32, each operation rounded on its
+ * own: per pixel, PBR Neutral (present.metal:22-35) of max(rgb * exposure,
+ * 0) from `rgba` (float copies of the half4 colour target), or, when
+ * debug_view, the drift heat map (present.metal:40-46) of the half4 debug
+ * target with `drift_budget`. Writes rgb before the half rounding. */
+void o32_present(const float* rgba, uint32_t count, float exposure, uint32_t debug_view, float drift_budget,
+                 float* rgb);
+
+/* Linear [0, 1] (clamped) to 8-bit sRGB, IEC 61966-2-1, rounded to
+ * nearest, in FP32. */
+void o32_srgb8(const float* v, uint64_t count, uint8_t* out);
 
 /* PBR Neutral (present.metal:22-35) on one colour. */
 void o_pbr_neutral(const double in[3], double out[3]);

@@ -321,3 +321,54 @@ void o32_resolve(const uint32_t* em, const int32_t* mo, const uint32_t* ma, uint
         vo[4 * index + 3] = 1.0f;
     }
 }
+
+/* present.metal:22-35 (pbrNeutral), FP32 */
+static void pbr_neutral32(float c[3]) {
+    const float start = 0.8f - 0.04f;
+    const float desat = 0.15f;
+    float x = fminf(c[0], fminf(c[1], c[2]));
+    float offset = x < 0.08f ? x - 6.25f * x * x : 0.04f;
+    for (int i = 0; i < 3; ++i) c[i] = c[i] - offset;
+    float peak = fmaxf(c[0], fmaxf(c[1], c[2]));
+    if (peak < start) return;
+    const float d = 1.0f - start;
+    float np = 1.0f - d * d / (peak + d - start);
+    float sc = np / peak;
+    for (int i = 0; i < 3; ++i) c[i] = c[i] * sc;
+    float g = 1.0f - 1.0f / (desat * (peak - np) + 1.0f);
+    for (int i = 0; i < 3; ++i) c[i] = c[i] + (np - c[i]) * g;
+}
+
+/* present.metal:40-46 (driftHeat), FP32 */
+static void drift_heat32(const float d[4], float budget, float out[3]) {
+    float t = fminf(fmaxf(d[0] / budget, 0.0f), 2.0f) * 0.5f;
+    float heat[3] = {t, 1.0f - fabsf(t - 0.5f) * 2.0f, 1.0f - t};
+    float shade = 0.2f + 0.8f * fminf(fmaxf(d[1] / (float)STEP_CAP_INTERACTIVE, 0.0f), 1.0f);
+    if (d[2] < 0.5f) shade = shade * 0.35f;
+    for (int i = 0; i < 3; ++i) out[i] = heat[i] * shade;
+}
+
+void o32_present(const float* rgba, uint32_t count, float exposure, uint32_t debug_view, float drift_budget,
+                 float* rgb) {
+    for (uint32_t i = 0; i < count; ++i) {
+        const float* h = rgba + 4 * (uint64_t)i;
+        float* o = rgb + 3 * (uint64_t)i;
+        if (debug_view) {
+            drift_heat32(h, drift_budget, o);
+        } else {
+            float c[3] = {fmaxf(h[0] * exposure, 0.0f), fmaxf(h[1] * exposure, 0.0f), fmaxf(h[2] * exposure, 0.0f)};
+            pbr_neutral32(c);
+            o[0] = c[0];
+            o[1] = c[1];
+            o[2] = c[2];
+        }
+    }
+}
+
+void o32_srgb8(const float* v, uint64_t count, uint8_t* out) {
+    for (uint64_t i = 0; i < count; ++i) {
+        float x = fminf(fmaxf(v[i], 0.0f), 1.0f);
+        float e = x <= 0.0031308f ? 12.92f * x : 1.055f * powf(x, 1.0f / 2.4f) - 0.055f;
+        out[i] = (uint8_t)lrintf(e * 255.0f);
+    }
+}

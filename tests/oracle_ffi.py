@@ -20,6 +20,8 @@ _dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
 _fp = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
 _u32p = np.ctypeslib.ndpointer(dtype=np.uint32, flags="C_CONTIGUOUS")
 _i32p = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+_ip = _i32p
+_u8p = np.ctypeslib.ndpointer(dtype=np.uint8, flags="C_CONTIGUOUS")
 
 
 class Settings(C.Structure):
@@ -158,6 +160,9 @@ def lib() -> C.CDLL:
                                 u32, i]),
         "o32_resolve": (None, [_u32p, _i32p, _u32p, u32, C.c_float, C.c_float, _fp, i, _fp, _fp, i]),
         "o_pbr_neutral": (None, [_dp, _dp]),
+        "o32_present": (None, [_fp, u32, C.c_float, u32, C.c_float, _fp]),
+        "o32_srgb8": (None, [_fp, C.c_uint64, _u8p]),
+        "o_bake_batch": (None, [_dp, i, C.POINTER(Settings), C.c_double, C.c_double, i, _dp, _ip, _ip, _ip, _dp, i]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(L, name)
@@ -332,3 +337,36 @@ def luminance(rgb: np.ndarray) -> np.ndarray:
 def side_ratio(lum: np.ndarray, width: int, height: int) -> float:
     lum = np.ascontiguousarray(lum, np.float64)
     return lib().o_side_ratio(lum, width, height)
+
+
+def present32(rgba_half: np.ndarray, exposure: float = 1.0, debug_view: bool = False,
+              drift_budget: float = 1e-4) -> np.ndarray:
+    """The tone-map kernel's output for half4 pixels (n x 4 float16): the
+    FP32 replica of PBR Neutral or the drift heat map, rounded to half as the
+    fragment returns it, then encoded to 8-bit sRGB; alpha 255."""
+    n = len(rgba_half)
+    src = np.ascontiguousarray(rgba_half.astype(np.float32))
+    rgb = np.zeros((n, 3), np.float32)
+    lib().o32_present(src, n, exposure, 1 if debug_view else 0, drift_budget, rgb)
+    halved = np.ascontiguousarray(rgb.astype(np.float16).astype(np.float32))
+    out = np.full((n, 4), 255, np.uint8)
+    codes = np.zeros((n, 3), np.uint8)
+    lib().o32_srgb8(halved, halved.size, codes)
+    out[:, :3] = codes
+    return out
+
+
+def bake_batch(probes: np.ndarray, settings: Settings, spacing: float, half_extent: float = 30.0,
+               capacity: int = 96, threads: int = 0):
+    """FP64 bake of rays launched at the camera: samples (n x capacity x 4),
+    counts, overflowed, falls_in, direction_depth (n x 4)."""
+    probes = np.ascontiguousarray(probes, np.float64)
+    n = len(probes)
+    samples = np.zeros((n, capacity, 4))
+    counts = np.zeros(n, np.int32)
+    over = np.zeros(n, np.int32)
+    falls = np.zeros(n, np.int32)
+    dd = np.zeros((n, 4))
+    lib().o_bake_batch(probes, n, C.byref(settings), spacing, half_extent, capacity, samples, counts, over, falls, dd,
+                       threads)
+    return samples, counts, over, falls, dd
