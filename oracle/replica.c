@@ -106,14 +106,16 @@ static void spawn32(uint32_t index, uint32_t event, const sim32* u, int from_dis
     memcpy(&p[7], &event, 4);
 }
 
-/* sim.metal:44-79 */
+/* sim.metal:44-79, with the angular frequency as sqrt(-k) = sqrt(g / r)
+ * (the reference divides circular_speed(r) = sqrt(r g) by r), as the
+ * kernel computes it. */
 static void step32(uint32_t i, const sim32* u, float* p) {
     float px = p[0], py = p[1], pz = p[2];
     float vx = p[3], vy = p[4], vz = p[5];
     for (uint32_t s = 0; s < SIM_SUBSTEPS; ++s) {
         float r = length3f(px, py, pz);
         float k = -gradf(r, u->potential) / r;
-        float omega = circular_speedf(r, u->potential) / r;
+        float omega = sqrtf(-k);
         vx = vx + px * k * u->dt;
         vy = vy + py * k * u->dt;
         vz = vz + pz * k * u->dt;
