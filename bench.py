@@ -444,7 +444,7 @@ def measure_passes(ctx, g, torch) -> dict:
         t = timed(lambda: vol.bin(ps, exact), pre=vol.clear)
         rate = 6.0 * deposits / t / 1e9
         peak, src = ((shared_peak, "gg_measure_shared_atomic_peak: scattered u32 shared atomics into a 9^3 "
-                                   "six-word tile") if edge else
+                                   "tile of six-word records padded to seven (all 32 banks)") if edge else
                      (atom_peak, "gg_measure_atomic_peak: scattered u32 REDs into a 128^3 six-word grid"))
         out["splat_bin_exact" if exact else "splat_bin_stochastic"] = {
             "workload": "1M settled particles (default preset) into 128^3", "us": t * 1e6,

@@ -48,18 +48,22 @@ __global__ void __launch_bounds__(256) red_kernel(uint32_t* sums, uint32_t recor
     }
 }
 
-// The same adds into a shared-memory tile of 9^3 six-word records (the
-// brick splat's tile at edge 8): the ceiling of its deposit loop.
+// The same adds into a shared-memory tile of 9^3 records (the brick splat's
+// tile at edge 8) laid out as the deposit lays it out: six words and a pad,
+// an odd stride, so that one word of records at random cells spreads over
+// all 32 banks. The result is the device's rate of scattered shared-memory
+// u32 atomic adds: the ceiling of the deposit loop.
 constexpr uint32_t kTileRecords = 9u * 9u * 9u;
+constexpr uint32_t kTileStride = 7u;
 
 __global__ void __launch_bounds__(256) shared_red_kernel(uint32_t* sink, uint32_t seed) {
-    __shared__ uint32_t tile[kTileRecords * 6u];
-    for (uint32_t w = threadIdx.x; w < kTileRecords * 6u; w += blockDim.x) tile[w] = 0u;
+    __shared__ uint32_t tile[kTileRecords * kTileStride];
+    for (uint32_t w = threadIdx.x; w < kTileRecords * kTileStride; w += blockDim.x) tile[w] = 0u;
     __syncthreads();
     uint32_t h = (blockIdx.x * blockDim.x + threadIdx.x) * 0x9E3779B1u + seed;
     for (int i = 0; i < kDeposits * 4; ++i) {
         h = h * 1664525u + 1013904223u;
-        uint32_t* rec = tile + 6u * __umulhi(h, kTileRecords);
+        uint32_t* rec = tile + kTileStride * __umulhi(h, kTileRecords);
         atomicAdd(rec + 0, 1u);
         atomicAdd(rec + 1, 1u);
         atomicAdd(rec + 2, 1u);

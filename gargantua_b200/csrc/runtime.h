@@ -137,7 +137,6 @@ struct gg_volume {
     // (0: direct global atomics) and particles per deposit work item.
     uint32_t brick_edge[2] = {0u, 8u};    // [stochastic, exact]; set per size by gg_volume_create
     uint32_t brick_chunk[2] = {0u, 1024u};
-    bool brick_merge[2] = {true, true};  // deposit: merge a warp's same-voxel lanes before the shared atomics
     void* brick_scratch = nullptr;  // counts, cursor, offsets, items, sorted slots, keys
     uint64_t brick_scratch_capacity = 0;
     bool brick_counts_zero = false;  // the counts region holds zeros (the count pass re-zeroes it)

@@ -134,14 +134,12 @@ __global__ void __launch_bounds__(256) bin_kernel(SplatArgs a) {
 //   scan     one block: brick offsets and work items (ceil(count / chunk)
 //            particles-chunks per brick);
 //   scatter  the histogram again from the stored keys, each block reserving
-//            its range of every brick with one atomic, then each particle's
-//            32-byte record (position and temperature; velocity and its
-//            index) written into brick order;
-//   deposit  one block per work item: the tile's six-word records zeroed in
-//            shared memory, the chunk's particle records streamed in order
-//            and deposited there with shared atomics (lanes of a warp that
-//            hit one voxel merged first, see deposit_corner), the non-zero
-//            words added to the sums with one global atomic each.
+//            its range of every brick with one atomic, then particle indices
+//            written into brick order;
+//   deposit  one block per work item: the tile's records (six words and a
+//            pad, see kTileStride) zeroed in shared memory, the chunk's particles deposited there with
+//            shared atomics, the non-zero words added to the sums with one
+//            global atomic each.
 // Integer sums do not depend on the order of the adds, so the grid equals
 // the direct kernel's bit for bit.
 
@@ -165,8 +163,7 @@ struct BrickArgs {
     uint32_t* offsets;   // [bricks + 1], exclusive scan of counts
     uint32_t* cursor;    // [bricks], reservation cursor
     uint32_t* items;     // [bricks + 1], exclusive scan of ceil(count / chunk)
-    float4* sorted_pos;  // [particleCount], particle records in brick order: (x, y, z, T)
-    float4* sorted_vel;  //   and (vx, vy, vz, particle slot as bits)
+    uint32_t* sorted;    // [particleCount], particle slots in brick order
     uint32_t* keys;      // [particleCount], each particle's brick (kOutside: none), from the count pass
 };
 
@@ -297,11 +294,7 @@ __global__ void __launch_bounds__(kBrickBlock) brick_scatter_kernel(BrickArgs a)
         const uint32_t key = a.keys[i];
         if (key >= a.bricks) continue;
         const uint32_t slot = atomicAdd(&hist[key], 1u);
-        if (slot < a.u.particleCount) {  // always: the counts came from the same keys
-            const float4 v = a.vel[i];
-            a.sorted_pos[slot] = a.pos[i];
-            a.sorted_vel[slot] = make_float4(v.x, v.y, v.z, __uint_as_float(i));
-        }
+        if (slot < a.u.particleCount) a.sorted[slot] = i;  // always: the counts came from the same keys
     }
 }
 
@@ -317,51 +310,21 @@ __device__ __forceinline__ uint32_t item_brick(const uint32_t* items, uint32_t b
     return lo;
 }
 
-// Threads of a deposit block. A 16^3 brick's 17^3 six-word tile takes 118 KB of
-// shared memory, so one block fills an SM: it gets 1024 threads to keep enough
+// Words per record in the deposit's shared tile: the six sums and one pad
+// word. With an odd stride the same word of records at random cells falls
+// on all 32 banks; with stride 6, 6 cell + c is even-offset and a warp's
+// atomics to one word reach only 16 banks, twice the conflicts.
+constexpr uint32_t kTileStride = 7;
+
+// Threads of a deposit block. A 16^3 brick's 17^3 tile of seven-word records
+// takes 138 KB of shared memory, so one block fills an SM: it gets 1024 threads to keep enough
 // shared atomics in flight; the smaller tiles fit several 256-thread blocks.
 template <uint32_t B> constexpr uint32_t deposit_threads() { return B == 16u ? 1024u : kBrickBlock; }
 
-constexpr uint32_t kNoCell = 0xFFFFFFFFu;
-
-// One corner's six words into the tile, called by every lane of the warp
-// together (cell kNoCell: this lane deposits nothing). With Merge, lanes
-// whose corners are the same tile cell are grouped by __match_any_sync, each
-// word is summed over the group by __reduce_add_sync, and the group's lowest
-// lane alone adds the sums: in a dense brick (many particles per voxel, the
-// max preset's inner disk) one shared atomic per group replaces one per
-// lane, where same-address atomics would serialise. Integer adds wrap
-// modulo 2^32 either way, so the tile words are the same.
-template <bool Merge>
-__device__ __forceinline__ void deposit_corner(uint32_t* tile, uint32_t cell, const Deposit& d, uint32_t lane) {
-    if constexpr (Merge) {
-        const uint32_t peers = __match_any_sync(0xffffffffu, cell);
-        uint32_t sum[6];
-#pragma unroll
-        for (int c = 0; c < 6; ++c) sum[c] = __reduce_add_sync(peers, d.w[c]);
-        if (cell != kNoCell && (uint32_t)(__ffs(peers) - 1) == lane) {
-            uint32_t* rec = tile + 6u * cell;
-#pragma unroll
-            for (int c = 0; c < 6; ++c) atomicAdd(rec + c, sum[c]);
-        }
-    } else {
-        if (cell != kNoCell) {
-            uint32_t* rec = tile + 6u * cell;
-#pragma unroll
-            for (int c = 0; c < 6; ++c) atomicAdd(rec + c, d.w[c]);
-        }
-    }
-}
-
-// The deposit of one work item. Every thread runs the same number of passes
-// (a warp-uniform loop; lanes past the chunk's end deposit nothing) so the
-// warp-wide merge sees whole warps. Each pass streams kGather records per
-// thread (block-strided, so a warp's loads are contiguous), all loaded
-// before any is deposited.
-template <uint32_t B, bool Merge>
+template <uint32_t B>
 __global__ void __launch_bounds__(deposit_threads<B>()) brick_deposit_kernel(BrickArgs a) {
     constexpr uint32_t T = B + 1;
-    constexpr uint32_t kWords = T * T * T * 6u;
+    constexpr uint32_t kCells = T * T * T;
     extern __shared__ uint32_t tile[];
     const uint32_t item = blockIdx.x;
     if (item >= a.items[a.bricks]) return;
@@ -371,77 +334,57 @@ __global__ void __launch_bounds__(deposit_threads<B>()) brick_deposit_kernel(Bri
     const uint32_t end = min(begin + a.chunk, a.offsets[b + 1]);
     const uint32_t bx = b % a.per_axis, by = (b / a.per_axis) % a.per_axis, bz = b / (a.per_axis * a.per_axis);
     const int ox = (int)(bx * B), oy = (int)(by * B), oz = (int)(bz * B);
-    for (uint32_t w = threadIdx.x; w < kWords; w += blockDim.x) tile[w] = 0u;
+    for (uint32_t w = threadIdx.x; w < kCells * kTileStride; w += blockDim.x) tile[w] = 0u;
     __syncthreads();
-    const uint32_t lane = threadIdx.x & 31u;
-    // The 16^3 deposit's 1024 threads have 64 registers each: two records in flight.
-    constexpr uint32_t kGather = B == 16u ? 2u : 4u;
-    for (uint32_t base = begin; base < end; base += kGather * blockDim.x) {
+    // kGather particles per thread per pass: their slots, then their
+    // positions and velocities, are loaded before any is deposited, so the
+    // random gathers overlap instead of following one another.
+    constexpr uint32_t kGather = 4;
+    for (uint32_t k0 = begin + threadIdx.x; k0 < end; k0 += kGather * blockDim.x) {
+        uint32_t idx[kGather];
         float4 pos[kGather], vel[kGather];
-        bool live[kGather];
 #pragma unroll
-        for (uint32_t g = 0; g < kGather; ++g) {
-            const uint32_t k = base + g * blockDim.x + threadIdx.x;
-            live[g] = k < end;
-            pos[g] = live[g] ? a.sorted_pos[k] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
-            vel[g] = live[g] ? a.sorted_vel[k] : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        for (uint32_t j = 0; j < kGather; ++j) {
+            const uint32_t k = k0 + j * blockDim.x;
+            idx[j] = k < end ? a.sorted[k] : kOutside;
         }
 #pragma unroll
-        for (uint32_t g = 0; g < kGather; ++g) {
-            Footprint f{};
+        for (uint32_t j = 0; j < kGather; ++j) {
+            if (idx[j] == kOutside) continue;
+            pos[j] = a.pos[idx[j]];
+            vel[j] = a.vel[idx[j]];
+        }
+#pragma unroll
+        for (uint32_t j = 0; j < kGather; ++j) {
+            if (idx[j] == kOutside) continue;
+            Footprint f;
             // Always inside and in this brick (the count pass put it here);
             // the test keeps every tile index in bounds regardless.
-            bool ok = live[g] && footprint(pos[g], a.u, f);
-            ok = ok && (uint32_t)(f.lx - ox) < B && (uint32_t)(f.ly - oy) < B && (uint32_t)(f.lz - oz) < B;
-            const float4 v = vel[g];
-            if (a.u.exactDeposit != 0u) {
+            if (!footprint(pos[j], a.u, f)) continue;
+            if ((uint32_t)(f.lx - ox) >= B || (uint32_t)(f.ly - oy) >= B || (uint32_t)(f.lz - oz) >= B) continue;
+            const float4 v = vel[j];
+            for_each_corner(f, a.u, a.first_index + idx[j], [&](int x, int y, int z, float w) {
+                Deposit d = deposit_values(w, f.energy, f.relative, v.x, v.y, v.z);
+                uint32_t* rec =
+                    tile + kTileStride * (((uint32_t)(z - oz) * T + (uint32_t)(y - oy)) * T + (uint32_t)(x - ox));
 #pragma unroll
-                for (uint32_t c = 0; c < CIC_CORNERS; ++c) {
-                    bool bxs = (c & 1u) != 0u, bys = (c & 2u) != 0u, bzs = (c & 4u) != 0u;
-                    float wx = bxs ? f.fx : 1.0f - f.fx;
-                    float wy = bys ? f.fy : 1.0f - f.fy;
-                    float wz = bzs ? f.fz : 1.0f - f.fz;
-                    float w = wx * wy * wz;
-                    uint32_t cell = kNoCell;
-                    Deposit d{};
-                    if (ok && w > 0.0f) {
-                        const uint32_t x = (uint32_t)((bxs ? f.hx : f.lx) - ox);
-                        const uint32_t y = (uint32_t)((bys ? f.hy : f.ly) - oy);
-                        const uint32_t z = (uint32_t)((bzs ? f.hz : f.lz) - oz);
-                        cell = (z * T + y) * T + x;
-                        d = deposit_values(w, f.energy, f.relative, v.x, v.y, v.z);
-                    }
-                    deposit_corner<Merge>(tile, cell, d, lane);
-                }
-            } else {
-                uint32_t cell = kNoCell;
-                Deposit d{};
-                if (ok) {
-                    const uint32_t index = __float_as_uint(v.w);
-                    uint4 h = pcg4d(make_uint4(a.first_index + index, a.u.frame, a.u.seed.x, a.u.seed.y));
-                    const uint32_t x = (uint32_t)((unit_float(h.x) < f.fx ? f.hx : f.lx) - ox);
-                    const uint32_t y = (uint32_t)((unit_float(h.y) < f.fy ? f.hy : f.ly) - oy);
-                    const uint32_t z = (uint32_t)((unit_float(h.z) < f.fz ? f.hz : f.lz) - oz);
-                    cell = (z * T + y) * T + x;
-                    d = deposit_values(1.0f, f.energy, f.relative, v.x, v.y, v.z);
-                }
-                deposit_corner<Merge>(tile, cell, d, lane);
-            }
+                for (int c = 0; c < 6; ++c) atomicAdd(rec + c, d.w[c]);
+            });
         }
     }
     __syncthreads();
     const uint32_t n = a.u.volumeSize;
-    for (uint32_t w = threadIdx.x; w < kWords; w += blockDim.x) {
-        const uint32_t val = tile[w];
-        if (!val) continue;
+    for (uint32_t w = threadIdx.x; w < kCells * 6u; w += blockDim.x) {
         const uint32_t cell = w / 6u, c = w - cell * 6u;
+        const uint32_t val = tile[cell * kTileStride + c];
+        if (!val) continue;
         const uint32_t tx = cell % T, ty = (cell / T) % T, tz = cell / (T * T);
         const uint32_t x = (uint32_t)ox + tx, y = (uint32_t)oy + ty, z = (uint32_t)oz + tz;
         if (x < n && y < n && z < n) atomicAdd(a.sums + 6ull * ((z * n + y) * n + x) + c, val);
     }
 }
 
-template <uint32_t B> constexpr uint32_t tile_bytes() { return (B + 1) * (B + 1) * (B + 1) * 6u * 4u; }
+template <uint32_t B> constexpr uint32_t tile_bytes() { return (B + 1) * (B + 1) * (B + 1) * kTileStride * 4u; }
 
 struct ResolveArgs {
     uint32_t* __restrict__ sums;
@@ -559,7 +502,7 @@ static int check_shape(const gg_volume* vol, uint32_t edge, uint32_t chunk) {
 // once per device.
 static int allow_shared(const void* kernel, int bytes, int device, int slot) {
     static std::mutex mu;
-    static int done[64][4] = {};  // slots: count, scatter, deposit, merging deposit
+    static int done[64][4] = {};
     if (bytes <= 48 * 1024 || device >= 64) return GG_OK;
     std::lock_guard<std::mutex> lock(mu);
     if (done[device][slot] >= bytes) return GG_OK;
@@ -572,17 +515,7 @@ static uint64_t align256(uint64_t x) { return (x + 255u) & ~255ull; }
 
 // gg_splat_bin with an explicit shape (caller holds the context lock and has
 // checked the arguments).
-template <uint32_t B>
-static int launch_deposit(const BrickArgs& a, uint32_t grid, bool merge, gg_context* ctx) {
-    const void* kernel = merge ? (const void*)brick_deposit_kernel<B, true> : (const void*)brick_deposit_kernel<B, false>;
-    GG_CHECK(allow_shared(kernel, (int)tile_bytes<B>(), ctx->device, merge ? 3 : 2));
-    if (merge) brick_deposit_kernel<B, true><<<grid, deposit_threads<B>(), tile_bytes<B>(), ctx->stream>>>(a);
-    else brick_deposit_kernel<B, false><<<grid, deposit_threads<B>(), tile_bytes<B>(), ctx->stream>>>(a);
-    return gg::launch_status("brick deposit");
-}
-
-static int splat_bin_shaped(gg_particles* ps, gg_volume* vol, const SplatUniforms* u, uint32_t edge, uint32_t chunk,
-                            bool merge) {
+static int splat_bin_shaped(gg_particles* ps, gg_volume* vol, const SplatUniforms* u, uint32_t edge, uint32_t chunk) {
     gg_context* ctx = vol->ctx;
     if (edge == 0u) {
         SplatArgs a{ps->pos, ps->vel, vol->sums, *u, ps->first_index};
@@ -594,11 +527,10 @@ static int splat_bin_shaped(gg_particles* ps, gg_volume* vol, const SplatUniform
     const uint32_t bricks = per * per * per;
     // counts (a fixed kMaxBricks words, whatever the shape, so that the
     // zeros the scan leaves behind stay counts), cursor, offsets, items,
-    // the sorted records (two float4 per particle), keys.
+    // sorted slots, keys.
     const uint64_t counts_bytes = align256(4ull * kMaxBricks);
     const uint64_t words = counts_bytes + align256(4ull * bricks) + align256(4ull * (bricks + 1u)) * 2u;
-    const uint64_t records = align256(16ull * ps->count);
-    const uint64_t bytes = words + 2u * records + align256(4ull * ps->count);
+    const uint64_t bytes = words + 2u * align256(4ull * ps->count);
     const uint64_t capacity_before = vol->brick_scratch_capacity;  // changes when the scratch is reallocated
     GG_CHECK(gg::ensure_capacity(ctx, &vol->brick_scratch, &vol->brick_scratch_capacity, bytes, "splat bricks"));
     char* base = static_cast<char*>(vol->brick_scratch);
@@ -624,9 +556,8 @@ static int splat_bin_shaped(gg_particles* ps, gg_volume* vol, const SplatUniform
     a.cursor = reinterpret_cast<uint32_t*>(base + counts_bytes);
     a.offsets = reinterpret_cast<uint32_t*>(base + counts_bytes + align256(4ull * bricks));
     a.items = reinterpret_cast<uint32_t*>(base + counts_bytes + align256(4ull * bricks) + align256(4ull * (bricks + 1u)));
-    a.sorted_pos = reinterpret_cast<float4*>(base + words);
-    a.sorted_vel = reinterpret_cast<float4*>(base + words + records);
-    a.keys = reinterpret_cast<uint32_t*>(base + words + 2u * records);
+    a.sorted = reinterpret_cast<uint32_t*>(base + words);
+    a.keys = reinterpret_cast<uint32_t*>(base + words + align256(4ull * ps->count));
     const int hist = (int)(4u * bricks);
     GG_CHECK(allow_shared((const void*)brick_count_kernel, hist, ctx->device, 0));
     GG_CHECK(allow_shared((const void*)brick_scatter_kernel, hist, ctx->device, 1));
@@ -642,9 +573,15 @@ static int splat_bin_shaped(gg_particles* ps, gg_volume* vol, const SplatUniform
     GG_CHECK(gg::launch_status("brick scatter"));
     // Work items number at most count / chunk + one per non-empty brick.
     const uint32_t grid = (ps->count + chunk - 1u) / chunk + bricks;
-    if (edge == 4u) return launch_deposit<4>(a, grid, merge, ctx);
-    if (edge == 8u) return launch_deposit<8>(a, grid, merge, ctx);
-    return launch_deposit<16>(a, grid, merge, ctx);
+    if (edge == 4u) {
+        brick_deposit_kernel<4><<<grid, deposit_threads<4>(), tile_bytes<4>(), ctx->stream>>>(a);
+    } else if (edge == 8u) {
+        brick_deposit_kernel<8><<<grid, deposit_threads<8>(), tile_bytes<8>(), ctx->stream>>>(a);
+    } else {
+        GG_CHECK(allow_shared((const void*)brick_deposit_kernel<16>, (int)tile_bytes<16>(), ctx->device, 2));
+        brick_deposit_kernel<16><<<grid, deposit_threads<16>(), tile_bytes<16>(), ctx->stream>>>(a);
+    }
+    return gg::launch_status("brick deposit");
 }
 
 static int check_splat(const gg_particles* ps, const gg_volume* vol, const SplatUniforms* u, const char* what) {
@@ -758,14 +695,7 @@ GG_API int gg_splat_bin(gg_particles* ps, gg_volume* vol, const SplatUniforms* u
     std::lock_guard<std::recursive_mutex> lock(ctx->mu);
     GG_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
     const int mode = u->exactDeposit ? 1 : 0;
-    return splat_bin_shaped(ps, vol, u, vol->brick_edge[mode], vol->brick_chunk[mode], vol->brick_merge[mode]);
-}
-
-GG_API int gg_volume_splat_merge(gg_volume* vol, int exact, int merge) {
-    if (!vol) return gg::fail(GG_ERR_INVALID_ARGUMENT, "gg_volume_splat_merge needs a volume.");
-    std::lock_guard<std::recursive_mutex> lock(vol->ctx->mu);
-    vol->brick_merge[exact ? 1 : 0] = merge != 0;
-    return GG_OK;
+    return splat_bin_shaped(ps, vol, u, vol->brick_edge[mode], vol->brick_chunk[mode]);
 }
 
 GG_API int gg_volume_splat_shape(gg_volume* vol, int exact, uint32_t brick_edge, uint32_t chunk) {
@@ -792,33 +722,26 @@ GG_API int gg_splat_autotune(gg_particles* ps, gg_volume* vol, const SplatUnifor
     GG_CUDA(cudaEventCreate(&e1), "autotune events");
     float best = 1e30f;
     uint32_t best_edge = 0, best_chunk = 0;
-    bool best_merge = false;
     int status = GG_OK;
     for (const auto& shape : kShapes) {
         if (check_shape(vol, shape[0], shape[1]) != GG_OK) continue;
-        // Brick shapes are timed with and without the warp merge of
-        // same-voxel lanes; the direct kernel has no merge.
-        for (int merge = 0; merge < (shape[0] ? 2 : 1) && status == GG_OK; ++merge) {
-            float total = 0.0f;
-            for (int rep = 0; rep < 4 && status == GG_OK; ++rep) {
-                status = gg_volume_clear(vol);
-                if (status == GG_OK) status = gg::cuda_status(cudaEventRecord(e0, ctx->stream), "autotune");
-                if (status == GG_OK) status = splat_bin_shaped(ps, vol, u, shape[0], shape[1], merge != 0);
-                if (status == GG_OK) status = gg::cuda_status(cudaEventRecord(e1, ctx->stream), "autotune");
-                if (status == GG_OK) status = gg::cuda_status(cudaEventSynchronize(e1), "autotune");
-                float ms = 0.0f;
-                if (status == GG_OK) status = gg::cuda_status(cudaEventElapsedTime(&ms, e0, e1), "autotune");
-                if (rep > 0) total += ms;  // the first run also grows the scratch
-            }
-            if (status != GG_OK) break;
-            if (total / 3.0f < best) {
-                best = total / 3.0f;
-                best_edge = shape[0];
-                best_chunk = shape[1];
-                best_merge = merge != 0;
-            }
+        float total = 0.0f;
+        for (int rep = 0; rep < 4 && status == GG_OK; ++rep) {
+            status = gg_volume_clear(vol);
+            if (status == GG_OK) status = gg::cuda_status(cudaEventRecord(e0, ctx->stream), "autotune");
+            if (status == GG_OK) status = splat_bin_shaped(ps, vol, u, shape[0], shape[1]);
+            if (status == GG_OK) status = gg::cuda_status(cudaEventRecord(e1, ctx->stream), "autotune");
+            if (status == GG_OK) status = gg::cuda_status(cudaEventSynchronize(e1), "autotune");
+            float ms = 0.0f;
+            if (status == GG_OK) status = gg::cuda_status(cudaEventElapsedTime(&ms, e0, e1), "autotune");
+            if (rep > 0) total += ms;  // the first run also grows the scratch
         }
         if (status != GG_OK) break;
+        if (total / 3.0f < best) {
+            best = total / 3.0f;
+            best_edge = shape[0];
+            best_chunk = shape[1];
+        }
     }
     cudaEventDestroy(e0);
     cudaEventDestroy(e1);
@@ -827,7 +750,6 @@ GG_API int gg_splat_autotune(gg_particles* ps, gg_volume* vol, const SplatUnifor
     const int mode = u->exactDeposit ? 1 : 0;
     vol->brick_edge[mode] = best_edge;
     vol->brick_chunk[mode] = best_chunk;
-    vol->brick_merge[mode] = best_merge;
     if (brick_edge) *brick_edge = best_edge;
     if (chunk) *chunk = best_chunk;
     if (best_ms) *best_ms = best;

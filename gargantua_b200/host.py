@@ -426,10 +426,6 @@ class Volume:
         """gg_volume_splat_shape: 0 = direct global atomics, else 4/8/16."""
         check(lib().gg_volume_splat_shape(self.handle, 1 if exact else 0, brick_edge, chunk))
 
-    def set_merge(self, exact: bool, merge: bool):
-        """gg_volume_splat_merge: merge a warp's same-voxel lanes in the brick deposit."""
-        check(lib().gg_volume_splat_merge(self.handle, 1 if exact else 0, 1 if merge else 0))
-
     def autotune(self, ps: "Particles", exact: bool = True) -> tuple[int, int, float]:
         """gg_splat_autotune: (brick edge, chunk, ms) of the fastest shape."""
         u = splat_uniforms(self.size, ps.count, ps.seed, self.frame, exact)

@@ -189,18 +189,10 @@ GG_API int gg_volume_write_sums(gg_volume* vol, const uint32_t* emission, const 
  * 2048 (exact) and 4096 (stochastic). */
 GG_API int gg_volume_splat_shape(gg_volume* vol, int exact, uint32_t brick_edge, uint32_t chunk);
 
-/* Whether the brick deposit of a mode merges the lanes of a warp that hit
- * the same voxel (__match_any_sync, then one shared atomic per group for
- * each word) before its shared atomics: fewer same-address atomics where
- * particles crowd a voxel, a little more work per corner elsewhere. The
- * sums are the same bit for bit either way. Default on; gg_splat_autotune
- * picks it with the shape. No reference counterpart. */
-GG_API int gg_volume_splat_merge(gg_volume* vol, int exact, int merge);
-
 /* Time gg_splat_bin under each shape on these particles (u->exactDeposit
- * selects the mode), brick shapes with and without the lane merge, and keep
- * the fastest for that mode. Outputs (each may be NULL): the chosen edge and
- * chunk and its time in ms. The sums are left zeroed. */
+ * selects the mode) and keep the fastest for that mode. Outputs (each may be
+ * NULL): the chosen edge and chunk and its time in ms. The sums are left
+ * zeroed. */
 GG_API int gg_splat_autotune(gg_particles* ps, gg_volume* vol, const SplatUniforms* u, uint32_t* brick_edge,
                              uint32_t* chunk, float* best_ms);
 
@@ -514,7 +506,8 @@ GG_API int gg_measure_fp32_peak(gg_context* ctx, double* tflops);
 GG_API int gg_measure_atomic_peak(gg_context* ctx, uint32_t records, double* gatomics);
 
 /* The same rate, in G adds/s, for 32-bit atomic adds into a shared-memory
- * tile of 9^3 six-word records (the brick splat's tile at edge 8). */
+ * tile of 9^3 six-word records padded to seven words, the brick deposit's
+ * layout (the brick splat's tile at edge 8). */
 GG_API int gg_measure_shared_atomic_peak(gg_context* ctx, double* gatomics);
 
 #ifdef __cplusplus

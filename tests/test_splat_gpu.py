@@ -122,19 +122,16 @@ def test_size_mismatch_is_an_argument_error(ctx, settled):
 SHAPES = [(0, 0), (4, 1024), (8, 64), (8, 2048), (16, 4096), (16, 100000)]
 
 
-@pytest.mark.parametrize("merge", [True, False], ids=["merge", "no-merge"])
 @pytest.mark.parametrize("shape", SHAPES, ids=[f"edge{e}-chunk{c}" for e, c in SHAPES])
 @pytest.mark.parametrize("size", [100, 128])
 @pytest.mark.parametrize("exact", [True, False])
-def test_every_splat_shape_is_bit_exact(ctx, settled, shape, size, exact, merge):
+def test_every_splat_shape_is_bit_exact(ctx, settled, shape, size, exact):
     """Direct atomics and the brick-privatised deposit (ragged last bricks at
-    100^3, many work items per brick at chunk 64), with and without the warp
-    merge of same-voxel lanes, give the replica's grids."""
+    100^3, many work items per brick at chunk 64) give the replica's grids."""
     import gargantua_b200 as g
 
     vol = g.Volume(ctx, size)
     vol.set_shape(exact, *shape)
-    vol.set_merge(exact, merge)
     vol.bin(settled, exact=exact, frame=5)
     em, mo, ma = vol.read_sums()
     rem, rmo, rma = O.deposit32(settled.read(), size, frame=5, exact=exact, seed=1)
@@ -143,13 +140,12 @@ def test_every_splat_shape_is_bit_exact(ctx, settled, shape, size, exact, merge)
     vol.close()
 
 
-@pytest.mark.parametrize("merge", [True, False], ids=["merge", "no-merge"])
 @pytest.mark.parametrize("exact", [True, False])
-def test_crowded_voxels_are_bit_exact(ctx, exact, merge):
+def test_crowded_voxels_are_bit_exact(ctx, exact):
     """The max preset's contention case scaled down: 70 % of 400k particles
     seeded from a surface density rising as r^-3 toward the ISCO, settled,
-    into 48^3, so hundreds of particles share each inner-disk voxel and
-    most warps of the deposit merge lanes."""
+    into 48^3, so hundreds of particles share each inner-disk voxel and the
+    deposit's atomics collide on the same words."""
     import gargantua_b200 as g
 
     ps = g.Particles(ctx, 400_000, seed=7)
@@ -158,7 +154,6 @@ def test_crowded_voxels_are_bit_exact(ctx, exact, merge):
     vol = g.Volume(ctx, 48)
     for edge, chunk in [(8, 4096), (16, 16384), (4, 1024)]:
         vol.set_shape(exact, edge, chunk)
-        vol.set_merge(exact, merge)
         vol.bin(ps, exact=exact, frame=3)
         em, mo, ma = vol.read_sums()
         vol.clear()
