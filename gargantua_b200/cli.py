@@ -15,10 +15,12 @@ GPU. Commands:
   5 warm-ups, 30 timed, mean / p50 / max), printed as one JSON object.
 * `version`, `constants` (the constant table as a C header).
 
+* `validate`: the goldens the device can be held to without the FP64
+  oracle, run by the C++ host (gargantua_b200/cli/gargantua validate, the
+  same library): exit 0 when all pass, 1 when one fails.
+
 The interactive window (MTKView, HUD, MetalFX) needs a display and has no
-counterpart here; running without a command says so and exits 2. The
-reference's `validate` runs goldens against its FP64 oracle, which here is
-test infrastructure: the goldens run as the `gpu` tests.
+counterpart here; running without a command says so and exits 2.
 """
 from __future__ import annotations
 
@@ -32,7 +34,7 @@ VERSION = "0.1.0"
 
 USAGE = ("usage: python -m gargantua_b200 [--preset small|default|max] [--particles N] [--volume 96|128|192|256] "
          "[--seed S] [--strategy march|bake] [--fps-cap 30|60] [--no-upscale] [--still out.png --width W --height H] "
-         "[--spin a] [--camera az,el,d] [--sequence N] | bench | version | constants")
+         "[--spin a] [--camera az,el,d] [--sequence N] | bench | validate | version | constants")
 
 PRESETS = {  # Presets.swift:72-93
     "small": (250_000, 96, 640, 360),
@@ -306,7 +308,24 @@ def constants_header() -> str:
         return fh.read()
 
 
-def run(o: Options) -> None:
+def validate(o: Options) -> int:
+    """Validate.run (Validate.swift:19-55) through the C++ host, which links
+    the same library: its table on stdout, its exit code returned."""
+    import subprocess
+
+    exe = os.path.join(os.path.dirname(os.path.abspath(__file__)), "cli", "gargantua")
+    if not os.path.exists(exe):
+        raise OperationalError(f"validate runs the C++ host, which is not built: make -C {os.path.dirname(exe)}.")
+    argv = [exe, "validate", "--preset", o.preset, "--seed", str(o.seed)]
+    if o.particles:
+        argv += ["--particles", str(o.particles)]
+    if o.volume:
+        argv += ["--volume", str(o.volume)]
+    sys.stdout.flush()
+    return subprocess.run(argv).returncode
+
+
+def run(o: Options) -> int:
     if o.command == "version":
         print(f"gargantua-b200 {VERSION}")
     elif o.command == "constants":
@@ -316,10 +335,10 @@ def run(o: Options) -> None:
     elif o.command == "bench":
         bench(o)
     elif o.command == "validate":
-        raise OperationalError("validate compares against the FP64 oracle, which ships with the tests: "
-                               "run python -m pytest tests -m gpu.")
+        return validate(o)
     else:
         raise OperationalError("The interactive window needs a display; use --still or bench.")
+    return 0
 
 
 def main(argv: list[str] | None = None) -> int:
@@ -330,7 +349,7 @@ def main(argv: list[str] | None = None) -> int:
         sys.stderr.write(f"{e}\n")
         return 64
     try:
-        run(o)
+        return run(o)
     except OperationalError as e:
         sys.stderr.write(f"{e}\n")
         return 2

@@ -16,8 +16,10 @@
 // advancing and the stochastic deposit (Still.swift:67-90). bench times
 // every pass of the preset's scene, each call waited to completion
 // (Bench.swift:27-45: 5 warm-ups, 30 timed; mean, p50, max), as one JSON
-// object. The interactive window needs a display and has no counterpart
-// here; validate runs as the GPU test suite, where the FP64 oracle lives.
+// object. validate holds the device to the goldens (Validate.swift:17-55)
+// and prints their table: exit 0 when every golden it runs passes, 1 when
+// one fails. The interactive window needs a display and has no counterpart
+// here.
 #include <algorithm>
 #include <cerrno>
 #include <chrono>
@@ -25,6 +27,7 @@
 #include <cstdint>
 #include <cstdio>
 #include <cstdlib>
+#include <cstdarg>
 #include <cstring>
 #include <functional>
 #include <string>
@@ -456,6 +459,395 @@ void bench(const Options& o) {
     std::printf("%s}\n", line.c_str());
 }
 
+// ------------------------------------------------------------- validate
+
+// A golden (Golden.swift:5-59): a claim, a kind of bar, the expected value
+// and tolerance, and named numeric parameters, embedded from the goldens'
+// JSON files at build time.
+struct GoldenFile {
+    const char* name;
+    const char* json;
+};
+
+const GoldenFile kGoldens[] = {
+#include "goldens_text.h"
+};
+
+// The text after `"key":` in a JSON object's text, or npos.
+size_t json_value_at(const std::string& text, const std::string& key) {
+    const std::string quoted = "\"" + key + "\"";
+    size_t at = text.find(quoted);
+    if (at == std::string::npos) return at;
+    at = text.find(':', at + quoted.size());
+    if (at == std::string::npos) return at;
+    ++at;
+    while (at < text.size() && (text[at] == ' ' || text[at] == '\n' || text[at] == '\t' || text[at] == '\r')) ++at;
+    return at;
+}
+
+struct Golden {
+    std::string name, claim, kind, parameters;
+    double expected = 0.0, tolerance = 0.0;
+
+    double number(const std::string& text, const std::string& key) const {
+        const size_t at = json_value_at(text, key);
+        char* end = nullptr;
+        const double v = at == std::string::npos ? 0.0 : std::strtod(text.c_str() + at, &end);
+        if (at == std::string::npos || end == text.c_str() + at)
+            throw OperationalError{"Golden " + name + " has no number " + key + "."};
+        return v;
+    }
+    std::string string(const std::string& text, const std::string& key) const {
+        const size_t at = json_value_at(text, key);
+        if (at == std::string::npos || text[at] != '"') throw OperationalError{"Golden " + name + " has no " + key + "."};
+        const size_t close = text.find('"', at + 1);
+        return text.substr(at + 1, close - at - 1);
+    }
+    double parameter(const std::string& key) const { return number(parameters, key); }
+    // Golden.passes (Golden.swift:47-53).
+    bool passes(double measured) const {
+        if (kind == "relative") return std::fabs(measured - expected) / std::fabs(expected) <= tolerance;
+        if (kind == "absolute") return std::fabs(measured - expected) <= tolerance;
+        return measured == expected;
+    }
+    std::string tolerance_text() const {
+        char buf[64];
+        if (kind == "relative") std::snprintf(buf, sizeof buf, "%.1f percent", tolerance * 100.0);
+        else if (kind == "absolute") std::snprintf(buf, sizeof buf, "%g", tolerance);
+        else std::snprintf(buf, sizeof buf, "bitwise");
+        return buf;
+    }
+};
+
+Golden load_golden(const std::string& name) {
+    for (const GoldenFile& f : kGoldens) {
+        if (name != f.name) continue;
+        Golden g;
+        g.name = name;
+        const std::string text = f.json;
+        g.claim = g.string(text, "claim");
+        g.kind = g.string(text, "kind");
+        g.expected = g.number(text, "expected");
+        g.tolerance = g.number(text, "tolerance");
+        const size_t at = json_value_at(text, "parameters");
+        if (at == std::string::npos) throw OperationalError{"Golden " + name + " has no parameters."};
+        g.parameters = text.substr(at, text.find('}', at) - at + 1);
+        return g;
+    }
+    throw OperationalError{"Golden " + name + " is missing from the embedded goldens."};
+}
+
+struct Row {
+    Golden golden;
+    std::string measured;
+    bool passed;
+    bool run;
+};
+
+std::string format(const char* fmt, ...) __attribute__((format(printf, 1, 2)));
+std::string format(const char* fmt, ...) {
+    char buf[256];
+    va_list ap;
+    va_start(ap, fmt);
+    std::vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    return buf;
+}
+
+// Probes.run's uniforms (Probes.swift:39-40): one-pixel image, no gas, no
+// redshift, no sphere jump; `still` picks the step policy.
+MarchUniforms probe_uniforms(bool still, float spin) {
+    Options cam;
+    MarchUniforms u = march_uniforms(cam, 1, 1, still, 1.0f);
+    u.redshift = 0u;
+    u.starSeed = 0u;
+    u.spin = spin;
+    return u;
+}
+
+RayProbe probe_of(const double origin[3], const double direction[3]) {
+    RayProbe p;
+    p.origin = {(float)origin[0], (float)origin[1], (float)origin[2]};
+    p.direction = {(float)direction[0], (float)direction[1], (float)direction[2]};
+    return p;
+}
+
+// Probes.aimed (Probes.swift:46-49): from `radius` on the x axis toward the
+// hole with impact parameter b.
+RayProbe aimed(double radius, double b, double direction_out[3] = nullptr) {
+    const double f = 1.0 - 2.0 / radius;
+    const double dphi = b * std::sqrt(f) / radius;
+    const double dr = -std::sqrt(std::max(0.0, 1.0 - dphi * dphi));
+    const double origin[3] = {radius, 0.0, 0.0}, direction[3] = {dr, dphi, 0.0};
+    if (direction_out) std::memcpy(direction_out, direction, sizeof direction);
+    return probe_of(origin, direction);
+}
+
+// Probes.cameraGrid (Probes.swift:52-66) for the default orbit camera.
+std::vector<RayProbe> camera_grid(uint32_t columns, uint32_t rows, double aspect) {
+    Options cam;
+    const MarchUniforms u = march_uniforms(cam, 1, 1, true, 1.0f);
+    const double tan_half = (double)std::tan((float)(50.0 * M_PI / 180.0) * 0.5f);
+    const double origin[3] = {u.cameraPosition.x, u.cameraPosition.y, u.cameraPosition.z};
+    std::vector<RayProbe> out;
+    for (uint32_t row = 0; row < rows; ++row)
+        for (uint32_t col = 0; col < columns; ++col) {
+            const double x = (2.0 * (col + 0.5) / columns - 1.0) * tan_half * aspect;
+            const double y = (1.0 - 2.0 * (row + 0.5) / rows) * tan_half;
+            double d[3] = {u.cameraForward.x + x * u.cameraRight.x + y * u.cameraUp.x,
+                           u.cameraForward.y + x * u.cameraRight.y + y * u.cameraUp.y,
+                           u.cameraForward.z + x * u.cameraRight.z + y * u.cameraUp.z};
+            const double len = std::sqrt(d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+            for (double& c : d) c /= len;
+            out.push_back(probe_of(origin, d));
+        }
+    return out;
+}
+
+std::vector<RayProbeResult> run_probes(gg_context* ctx, const MarchUniforms& u, const std::vector<RayProbe>& probes) {
+    std::vector<RayProbeResult> out(probes.size());
+    check(gg_probe(ctx, &u, probes.data(), out.data(), (uint32_t)probes.size(), GG_PRECISION_PLAIN));
+    return out;
+}
+
+// DiskEdge.innerEdge (DiskEdge.swift:14-43): Sigma r^(3/2) binned over the
+// fit window, a least-squares line, extrapolated to zero.
+double disk_inner_edge(const std::vector<double>& radii, double width, double inner, double outer) {
+    const int count = (int)std::lround((outer - inner) / width);
+    std::vector<double> counts(count, 0.0);
+    for (double r : radii)
+        if (r >= inner && r < outer) counts[std::min((int)((r - inner) / width), count - 1)] += 1.0;
+    double sx = 0.0, sy = 0.0, sxx = 0.0, sxy = 0.0;
+    for (int k = 0; k < count; ++k) {
+        const double x = inner + (k + 0.5) * width;
+        const double y = counts[k] / (2.0 * M_PI * x * width) * std::pow(x, 1.5);
+        sx += x;
+        sy += y;
+        sxx += x * x;
+        sxy += x * y;
+    }
+    const double n = count;
+    const double slope = (n * sxy - sx * sy) / (n * sxx - sx * sx);
+    const double intercept = (sy - slope * sx) / n;
+    return -intercept / slope;
+}
+
+uint64_t settled_checksum(gg_context* ctx, const Options& o, uint32_t particles, uint32_t dispatches) {
+    gg_particles* ps = nullptr;
+    check(gg_particles_create(ctx, particles, o.seed, PotentialPaczynskiWiita, &ps));
+    uint64_t sum = 0;
+    int status = gg_particles_seed(ps);
+    if (status == GG_OK) status = gg_particles_step(ps, dispatches);
+    if (status == GG_OK) status = gg_particles_checksum(ps, &sum);
+    gg_particles_destroy(ps);
+    check(status);
+    return sum;
+}
+
+// An IEEE binary16 value (the march targets' rgba16f words).
+double half_to_double(uint16_t h) {
+    const int exponent = (h >> 10) & 0x1f, mantissa = h & 0x3ff;
+    const double sign = (h & 0x8000) ? -1.0 : 1.0;
+    if (exponent == 0) return sign * std::ldexp((double)mantissa, -24);
+    if (exponent == 31) return mantissa ? NAN : sign * INFINITY;
+    return sign * std::ldexp((double)(mantissa | 0x400), exponent - 25);
+}
+
+// Validate.jump's render (Validate.swift:320-347): still policy, no stars,
+// with or without the sphere jump; luminance per pixel.
+std::vector<double> render_luminance(Scene& s, uint32_t w, uint32_t h, bool jump) {
+    Options cam;
+    MarchUniforms u = march_uniforms(cam, w, h, true, DRIFT_BUDGET_STILL);
+    u.starBrightness = 0.0f;
+    u.starSeed = 0u;
+    if (jump) check(gg_tables_update(s.ctx, (float)cam.distance, &u));
+    gg_targets* t = nullptr;
+    check(gg_targets_create(s.ctx, w, h, &t));
+    std::vector<uint16_t> color((size_t)w * h * 4);
+    int status = gg_march(s.ctx, s.vol, &u, t, GG_PRECISION_PLAIN, nullptr);
+    if (status == GG_OK) status = gg_targets_read(t, color.data(), nullptr, nullptr, nullptr);
+    gg_targets_destroy(t);
+    check(status);
+    std::vector<double> lum((size_t)w * h);
+    for (size_t i = 0; i < lum.size(); ++i) {
+        double rgb[3];
+        for (int c = 0; c < 3; ++c) rgb[c] = half_to_double(color[4 * i + c]);
+        lum[i] = 0.2126 * rgb[0] + 0.7152 * rgb[1] + 0.0722 * rgb[2];
+    }
+    return lum;
+}
+
+// The Kerr shadow's equatorial edge on one side, as L / E of the launch at
+// the boundary: the reference's bisection through single-ray probes
+// (Validate.swift:352-365), and the same boundary bisected in FP64 on the
+// device (gg_capture_boundary).
+double kerr_xi_of(gg_context* ctx, const MarchUniforms& u, double radius, double side, double aim) {
+    const double origin[3] = {radius, 0.0, 0.0}, direction[3] = {-1.0, side * aim, 0.0};
+    const RayProbeResult r = run_probes(ctx, u, {probe_of(origin, direction)})[0];
+    return (double)r.angularMomentum / (double)r.energy;
+}
+
+double kerr_xi_probes(gg_context* ctx, const MarchUniforms& u, double radius, double side, int iterations) {
+    double low = 0.0, high = 12.0 / radius;
+    for (int i = 0; i < iterations; ++i) {
+        const double aim = 0.5 * (low + high);
+        const double origin[3] = {radius, 0.0, 0.0}, direction[3] = {-1.0, side * aim, 0.0};
+        const RayProbeResult r = run_probes(ctx, u, {probe_of(origin, direction)})[0];
+        if (r.outcome == RayCaptured) low = aim;
+        else high = aim;
+    }
+    return kerr_xi_of(ctx, u, radius, side, 0.5 * (low + high));
+}
+
+double kerr_xi_fp64(gg_context* ctx, const MarchUniforms& u, double radius, double side) {
+    const double origin[3] = {radius, 0.0, 0.0}, base[3] = {-1.0, 0.0, 0.0}, axis[3] = {0.0, side, 0.0};
+    double t = 0.0;
+    check(gg_capture_boundary(ctx, &u, origin, base, axis, 0.0, 12.0 / radius, 1024, 4, &t));
+    return kerr_xi_of(ctx, u, radius, side, t);
+}
+
+// Validate.run (Validate.swift:19-55): the default preset's disk settled for
+// the isco golden, then each golden in the reference's order. Parity,
+// beaming and sky compare against the FP64 oracle, which is test
+// infrastructure here and is not linked into this program: those rows
+// report that the test suite runs them (tests/test_goldens_gpu.py) and do
+// not decide the exit code.
+int validate(const Options& o) {
+    Scene s;
+    s.particles = o.particles ? o.particles : o.preset->particles;
+    s.size = o.volume ? o.volume : o.preset->volume;
+    check(gg_context_create(0, 0, &s.ctx));
+    const Golden isco = load_golden("isco");
+    check(gg_particles_create(s.ctx, s.particles, o.seed, PotentialPaczynskiWiita, &s.ps));
+    check(gg_particles_seed(s.ps));
+    check(gg_particles_step(s.ps, (uint32_t)isco.parameter("settlingSteps") / SIM_SUBSTEPS));
+    check(gg_volume_create(s.ctx, s.size, &s.vol));
+    const char* order[] = {"isco", "determinism", "shadow", "deflection", "conservation_interactive",
+                           "conservation_still", "parity", "beaming", "sky", "jump", "shadow_kerr"};
+    std::vector<Row> rows;
+    for (const char* name : order) {
+        const Golden g = load_golden(name);
+        const std::string n = name;
+        if (n == "isco") {
+            std::vector<Particle> parts(s.particles);
+            check(gg_particles_read(s.ps, parts.data(), s.particles));
+            std::vector<double> radii(parts.size());
+            for (size_t i = 0; i < parts.size(); ++i)
+                radii[i] = std::sqrt((double)parts[i].position.x * parts[i].position.x +
+                                     (double)parts[i].position.y * parts[i].position.y);
+            const double edge =
+                disk_inner_edge(radii, g.parameter("binWidth"), g.parameter("fitInner"), g.parameter("fitOuter"));
+            rows.push_back({g, format("r = %.3f", edge), g.passes(edge), true});
+        } else if (n == "determinism") {
+            const uint32_t d = (uint32_t)g.parameter("steps") / SIM_SUBSTEPS;
+            const uint64_t a = settled_checksum(s.ctx, o, s.particles, d), b = settled_checksum(s.ctx, o, s.particles, d);
+            rows.push_back({g, format("%016llx vs %016llx", (unsigned long long)a, (unsigned long long)b), a == b, true});
+        } else if (n == "shadow") {
+            double low = g.parameter("bracketLow"), high = g.parameter("bracketHigh");
+            const double radius = g.parameter("launchRadius");
+            const int per = (int)g.parameter("raysPerRound");
+            const MarchUniforms u = probe_uniforms(true, 0.0f);
+            double measured = -1.0;
+            for (int round = 0; round < (int)g.parameter("rounds") && measured < 0.0; ++round) {
+                std::vector<double> values;
+                std::vector<RayProbe> probes;
+                for (int i = 0; i < per; ++i) {
+                    values.push_back(low + (high - low) * ((i + 0.5) / per));
+                    probes.push_back(aimed(radius, values.back()));
+                }
+                const std::vector<RayProbeResult> res = run_probes(s.ctx, u, probes);
+                int exhausted = -1, escaped = per;
+                for (int i = per - 1; i >= 0; --i) {
+                    if (res[i].outcome == RayExhausted) exhausted = i;
+                    if (res[i].outcome == RayEscaped) escaped = i;
+                }
+                if (exhausted >= 0) {
+                    measured = values[exhausted];
+                    break;
+                }
+                const double new_low = escaped > 0 ? values[escaped - 1] : low;
+                const double new_high = escaped < per ? values[escaped] : high;
+                low = new_low;
+                high = new_high;
+            }
+            const double critical = measured >= 0.0 ? measured : 0.5 * (low + high);
+            rows.push_back({g, format("b = %.4f", critical), g.passes(critical), true});
+        } else if (n == "deflection") {
+            const double radius = g.parameter("launchRadius");
+            MarchUniforms u = probe_uniforms(true, 0.0f);
+            u.geodesic.stepMax = INFINITY;
+            u.geodesic.escapeRadius = (float)radius;
+            double a[3];
+            const RayProbe launch = aimed(radius, g.parameter("impactParameter"), a);
+            const RayProbeResult r = run_probes(s.ctx, u, {launch})[0];
+            const double d[3] = {r.direction.x, r.direction.y, r.direction.z};
+            const double c[3] = {a[1] * d[2] - a[2] * d[1], a[2] * d[0] - a[0] * d[2], a[0] * d[1] - a[1] * d[0]};
+            const double angle =
+                std::atan2(std::sqrt(c[0] * c[0] + c[1] * c[1] + c[2] * c[2]), a[0] * d[0] + a[1] * d[1] + a[2] * d[2]);
+            const bool escaped = r.outcome == RayEscaped;
+            rows.push_back({g, format("%.6f rad%s", angle, escaped ? "" : " (ray did not escape)"),
+                            g.passes(angle) && escaped, true});
+        } else if (n == "conservation_interactive" || n == "conservation_still") {
+            const bool still = n == "conservation_still";
+            const std::vector<RayProbe> grid =
+                camera_grid((uint32_t)g.parameter("columns"), (uint32_t)g.parameter("rows"), 960.0 / 540.0);
+            const std::vector<RayProbeResult> res = run_probes(s.ctx, probe_uniforms(still, 0.0f), grid);
+            double worst = 0.0;
+            int exhausted = 0;
+            for (const RayProbeResult& r : res) {
+                worst = std::max(worst, (double)r.drift);
+                exhausted += r.outcome == RayExhausted ? 1 : 0;
+            }
+            rows.push_back({g, format("max drift %.2e, %d of %zu rays exhausted", worst, exhausted, res.size()),
+                            g.passes(worst), true});
+        } else if (n == "jump") {
+            // The volume as the reference's run leaves it before the jump
+            // golden: the settled disk, splatted exactly (Validate.swift:262-266).
+            s.splat(o.seed, true);
+            const uint32_t w = (uint32_t)g.parameter("width"), h = (uint32_t)g.parameter("height");
+            const std::vector<double> full = render_luminance(s, w, h, false), jumped = render_luminance(s, w, h, true);
+            double difference = 0.0, total = 0.0;
+            for (size_t i = 0; i < full.size(); ++i) {
+                difference += std::fabs(full[i] - jumped[i]);
+                total += full[i];
+            }
+            const double measured = total > 0.0 ? difference / total : 1.0;
+            rows.push_back({g, format("mean relative difference %.2e", measured), g.passes(measured), true});
+        } else if (n == "shadow_kerr") {
+            const double spin = g.parameter("spin"), radius = g.parameter("launchRadius");
+            const MarchUniforms u = probe_uniforms(true, (float)spin);
+            const int iterations = (int)g.parameter("iterations");
+            const double gpu = std::fabs(kerr_xi_probes(s.ctx, u, radius, -1.0, iterations) /
+                                         kerr_xi_probes(s.ctx, u, radius, 1.0, iterations));
+            const double fp64 = std::fabs(kerr_xi_fp64(s.ctx, u, radius, -1.0) / kerr_xi_fp64(s.ctx, u, radius, 1.0));
+            const double measured = gpu / fp64;
+            rows.push_back({g, format("gpu %.4f vs FP64 bisection %.4f, ratio %.4f", gpu, fp64, measured),
+                            g.passes(measured), true});
+        } else {
+            rows.push_back({g, "needs the FP64 oracle: run by the test suite", true, false});
+        }
+    }
+    // Validate.print (Validate.swift:388-397).
+    size_t wn = 6, wc = 5, wm = 8;
+    for (const Row& r : rows) {
+        wn = std::max(wn, r.golden.name.size());
+        wc = std::max(wc, r.golden.claim.size());
+        wm = std::max(wm, r.measured.size());
+    }
+    auto pad = [](const std::string& t, size_t w) { return t + std::string(w > t.size() ? w - t.size() : 0, ' '); };
+    std::printf("validation on CUDA device 0\n");
+    std::printf("%s  %s  %s  tolerance    status\n", pad("golden", wn).c_str(), pad("claim", wc).c_str(),
+                pad("measured", wm).c_str());
+    bool all = true;
+    for (const Row& r : rows) {
+        all = all && r.passed;
+        std::printf("%s  %s  %s  %s  %s\n", pad(r.golden.name, wn).c_str(), pad(r.golden.claim, wc).c_str(),
+                    pad(r.measured, wm).c_str(), pad(r.golden.tolerance_text(), 11).c_str(),
+                    !r.run ? "skipped" : (r.passed ? "pass" : "FAIL"));
+    }
+    return all ? 0 : 1;
+}
+
 int run(const Options& o) {
     if (o.command == "version") {
         std::printf("gargantua-b200 %s\n", kVersion);
@@ -466,8 +858,7 @@ int run(const Options& o) {
     } else if (o.command == "bench") {
         bench(o);
     } else if (o.command == "validate") {
-        throw OperationalError{"validate compares against the FP64 oracle, which ships with the tests: "
-                               "run python -m pytest tests -m gpu."};
+        return validate(o);
     } else {
         throw OperationalError{"The interactive window needs a display; use --still or bench."};
     }

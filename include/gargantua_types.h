@@ -13,12 +13,21 @@
  * 8-byte alignment, simd_float4 is 16/16 and simd_float4x4 is 64/16. On
  * Apple platforms the real header is used; elsewhere the shim below gives
  * structs of exactly those sizes and alignments.
+ *
+ * A host that has already included its own ShaderTypes.h (its include
+ * guard GARGANTUA_SHADER_TYPES_H is defined) keeps its types: the
+ * definitions below are skipped, the library's entry points take the host's
+ * structs by the same names, and the layout pins at the end check the
+ * host's header instead. A Swift host importing both its ShaderTypes module
+ * and this library's module then sees one set of types.
  */
 #ifndef GARGANTUA_TYPES_H
 #define GARGANTUA_TYPES_H
 
 #include <stddef.h>
 #include <stdint.h>
+
+#ifndef GARGANTUA_SHADER_TYPES_H
 
 #if defined(__APPLE__) && !defined(GG_FORCE_SIMD_SHIM)
 #include <simd/simd.h>
@@ -179,6 +188,8 @@ typedef struct {
     uint32_t exhausted;
     uint32_t captured;
 } MarchCounters;
+
+#endif /* GARGANTUA_SHADER_TYPES_H */
 
 /* Layout pins, the sizes and offsets ShaderTypes.h produces under Apple's
  * simd alignment rules. */

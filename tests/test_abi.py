@@ -72,6 +72,32 @@ def test_c_header_compiles_with_layout_asserts(tmp_path):
         assert subprocess.run([str(exe)]).returncode == 0
 
 
+def test_a_host_shadertypes_header_included_first_is_used(tmp_path):
+    """A host that includes its own ShaderTypes.h before gargantua.h keeps
+    its structs (the header skips its definitions when the host's include
+    guard is set) and the layout pins check the host's structs. The host
+    header here is this header's own definitions with one field renamed, so
+    the program compiles only if the host's MarchUniforms is the one in
+    use."""
+    import subprocess
+
+    text = open(os.path.join(ROOT, "include", "gargantua_types.h")).read()
+    body = text[text.index("#ifndef GARGANTUA_SHADER_TYPES_H") + len("#ifndef GARGANTUA_SHADER_TYPES_H"):
+                text.index("#endif /* GARGANTUA_SHADER_TYPES_H */")]
+    assert "float opacityScale;" in body
+    host = ("#ifndef GARGANTUA_SHADER_TYPES_H\n#define GARGANTUA_SHADER_TYPES_H\n#include <stdint.h>\n"
+            + body.replace("float opacityScale;", "float hostOpacity;") + "\n#endif\n")
+    (tmp_path / "ShaderTypes.h").write_text(host)
+    src = tmp_path / "host.c"
+    src.write_text('#include "ShaderTypes.h"\n#include "gargantua.h"\n'
+                   "int main(void) { MarchUniforms u; u.hostOpacity = 0.5f; return (int)sizeof u - 192; }\n")
+    exe = tmp_path / "host"
+    r = subprocess.run(["/usr/bin/gcc", "-std=c11", str(src), "-I", str(tmp_path), "-I", os.path.join(ROOT, "include"),
+                        "-o", str(exe)], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    assert subprocess.run([str(exe)]).returncode == 0
+
+
 def test_constants_match_the_reference_table():
     """Every constant in the reference's generated header carries the same
     value in include/gargantua_constants.h (StyleTests.swift:40-44 keeps the
@@ -166,3 +192,20 @@ def test_python_argument_counts_match_the_prototypes():
              if n in counts and len(args) != counts[n]}
     assert not wrong, wrong
     assert set(_lib.SIGNATURES) <= set(counts), set(_lib.SIGNATURES) - set(counts)
+
+
+def test_swift_module_files_bind_the_header():
+    """The Swift system-library module (swift/): its module map's umbrella
+    header reaches include/gargantua.h and links the library, and every gg_
+    function the sample host calls is declared in the header. (No Swift
+    toolchain here compiles it.)"""
+    swift = os.path.join(ROOT, "swift")
+    modulemap = open(os.path.join(swift, "GargantuaCUDA", "module.modulemap")).read()
+    assert 'header "shim.h"' in modulemap and 'link "gargantua_b200"' in modulemap
+    shim = open(os.path.join(swift, "GargantuaCUDA", "shim.h")).read()
+    target = re.search(r'#include "([^"]*gargantua\.h)"', shim).group(1)
+    assert os.path.exists(os.path.normpath(os.path.join(swift, "GargantuaCUDA", target)))
+    header = open(os.path.join(ROOT, "include", "gargantua.h")).read()
+    declared = set(re.findall(r"GG_API\s+(?:const\s+)?\w+\s*\**\s*(gg_\w+)\(", header))
+    called = set(re.findall(r"\b(gg_\w+)\(", open(os.path.join(swift, "Sources", "gg-still", "main.swift")).read()))
+    assert called and called <= declared, called - declared

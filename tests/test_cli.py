@@ -49,9 +49,10 @@ def test_camera_clamps_elevation():
     assert cam.elevation == 1.5 and cam.distance == 30.0 and cam.azimuth == 0.5
 
 
-def _run(*args):
+def _run(*args, env=None):
     return subprocess.run([sys.executable, "-m", "gargantua_b200", *args], capture_output=True, text=True,
-                          cwd=cli.os.path.dirname(cli.os.path.dirname(cli.__file__)))
+                          cwd=cli.os.path.dirname(cli.os.path.dirname(cli.__file__)),
+                          env=None if env is None else {**cli.os.environ, **env})
 
 
 def test_exit_codes_and_simple_commands():
@@ -63,8 +64,8 @@ def test_exit_codes_and_simple_commands():
     assert r.returncode == 0 and "#define STEP_CAP_STILL" in r.stdout
     r = _run()
     assert r.returncode == 2 and "display" in r.stderr
-    r = _run("validate")
-    assert r.returncode == 2 and "pytest" in r.stderr
+    r = _run("validate", env={"CUDA_VISIBLE_DEVICES": ""})
+    assert r.returncode == 2 and "No CUDA device" in r.stderr
 
 
 def test_request_output_buffers_are_checked_before_the_library_writes():
