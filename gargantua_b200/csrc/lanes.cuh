@@ -160,6 +160,7 @@ template <typename R> struct SLane {
     V3<R> e1, e2;
     R energy, angular_momentum;  // launch values (the reference's ray.energy, ray.angularMomentum)
     double e0, l0;               // E and L of the state integration starts from, in double
+    float pre_drift;             // renormalised lanes: max over steps of the drift before projection
     float3 color;
     float transmittance, travelled, weighted_depth, depth_weight;
     V3<R> previous;
@@ -204,6 +205,7 @@ __device__ __forceinline__ bool s_init(SLane<R>& l, V3<R> origin, V3<R> directio
     double r0 = (double)l.s.r;
     l.e0 = (1.0 - 2.0 / r0) * (double)l.s.vd - (double)l.s.rd;
     l.l0 = r0 * r0 * (double)l.s.pd;
+    l.pre_drift = 0.0f;
     l.color = make_float3(0.0f, 0.0f, 0.0f);
     l.transmittance = 1.0f;
     l.travelled = l.weighted_depth = l.depth_weight = 0.0f;
@@ -231,9 +233,59 @@ template <typename R, bool Comp> __device__ __forceinline__ void s_advance(SStat
     comp_addT<Comp>(s.pd, c.pd, inc.pd);
 }
 
+// value + error word of a compensated component, set from a double.
+__device__ __forceinline__ void set_pair(float& x, float& e, double v) {
+    x = (float)v;
+    e = (float)(v - (double)x);
+}
+__device__ __forceinline__ void set_pair(double& x, double& e, double v) {
+    x = v;
+    e = 0.0;
+}
+
+// Hamiltonian-constraint renormalisation of a Schwarzschild state (the
+// constraint of Schwarzschild.swift:115-117): with L0 and E0 the values the
+// integration started from, set phiDot = L0 / r^2 and rDot, vDot on the
+// null cone -f vDot^2 + 2 vDot rDot + r^2 phiDot^2 = 0 with E = f vDot -
+// rDot = E0: rDot = sign(rDot) sqrt(E0^2 - f L0^2 / r^2), and vDot = (E0 +
+// rDot) / f, written as (L0^2 / r^2) / (E0 - rDot) for an ingoing ray so
+// that nothing cancels near the horizon. rDot is only replaced when the root
+// is real and within kProjectLimit of |rDot|: near a radial turning point
+// (rDot ~ 0) a small error in the root is a large change of direction, and
+// projecting there moved endpoints away from the FP64 integration; there
+// rDot is kept and vDot follows from E0. Evaluated in double from value
+// plus error word. Before projecting, the state's drift against E0, L0
+// joins the lane's running maximum, so the reported drift is the
+// integrator's own per-step error, not the roundoff the projection leaves.
+constexpr double kProjectLimit = 1e-3;
+
+template <typename R> __device__ __forceinline__ void s_project(SLane<R>& l) {
+    const double r = (double)l.s.r + (double)l.c.r;
+    const double f = 1.0 - 2.0 / r;
+    const double vd = (double)l.s.vd + (double)l.c.vd, rd = (double)l.s.rd + (double)l.c.rd;
+    const double pd = (double)l.s.pd + (double)l.c.pd;
+    const double pre = fmax(fabs(f * vd - rd - l.e0) / fabs(l.e0), fabs(r * r * pd - l.l0) / fmax(fabs(l.l0), 1e-3));
+    l.pre_drift = fmaxf(l.pre_drift, (float)pre);
+    const double inv_r2 = 1.0 / (r * r);
+    const double l2 = l.l0 * l.l0 * inv_r2;
+    const double disc = l.e0 * l.e0 - f * l2;
+    double rd_new = rd, vd_new = (l.e0 + rd) / f;
+    if (disc > 0.0) {
+        const double root = sqrt(disc);
+        if (fabs(root - fabs(rd)) <= kProjectLimit * fabs(rd)) {
+            rd_new = rd < 0.0 ? -root : root;
+            vd_new = rd < 0.0 ? l2 / (l.e0 + root) : (l.e0 + root) / f;
+        }
+    }
+    set_pair(l.s.pd, l.c.pd, l.l0 * inv_r2);
+    set_pair(l.s.rd, l.c.rd, rd_new);
+    set_pair(l.s.vd, l.c.vd, vd_new);
+}
+
 // One iteration of marchRay's loop (march.metal:65-106). Returns true when
 // the ray ended (captured, escaped, left the sphere or hit the step cap).
-template <typename R, bool Comp = true>
+// Project: renormalise the state after each step (s_project).
+template <typename R, bool Comp = true, bool Project = false>
 __device__ __forceinline__ bool s_step(SLane<R>& l, const MarchUniforms& u, cudaTextureObject_t em,
                                        cudaTextureObject_t vel, bool gather) {
     const GeodesicSettings& g = u.geodesic;
@@ -249,6 +301,7 @@ __device__ __forceinline__ bool s_step(SLane<R>& l, const MarchUniforms& u, cuda
         l.c = before_c;
         s_advance<R, Comp>(l.s, l.c, h * frac);
     }
+    if constexpr (Project) s_project(l);
     R sn, cs;
     V3<R> position = s_position(l, &sn, &cs);
     V3<R> d = position - l.previous;
@@ -286,7 +339,7 @@ template <typename R> __device__ __forceinline__ float s_drift(const SLane<R>& l
     double lm = r * r * ((double)l.s.pd + (double)l.c.pd);
     double ed = fabs(e - l.e0) / fabs(l.e0);
     double ld = fabs(lm - l.l0) / fmax(fabs(l.l0), 1e-3);
-    return (float)fmax(ed, ld);
+    return fmaxf(l.pre_drift, (float)fmax(ed, ld));
 }
 
 template <typename R> __device__ __forceinline__ bool s_falls_in(const SLane<R>& l) {
@@ -597,10 +650,42 @@ __device__ __forceinline__ void k_init(KLane<R>& l, float3 origin, float3 direct
     k_init(l, v3_of<R>(origin), v3_of<R>(direction), u);
 }
 
+// Hamiltonian-constraint renormalisation of a Kerr state: |p_r| solved
+// from 2 Sigma H = 0 (Kerr.h:39-50), Delta p_r^2 = P^2 / Delta - p_theta^2
+// - g(theta), where that is positive (outside the outer horizon) and the
+// new |p_r| is within kProjectLimit of the old (not near a radial turning
+// point, as for Schwarzschild), keeping p_r's sign. E and L are parameters here
+// and do not drift; p_theta and the Carter constant are left as integrated.
+// Before projecting, the state's gauge (the larger of |Q - Q0| and |2 Sigma
+// H| / max(r^2, 1)) joins the lane's running maximum, so the reported drift
+// is the integrator's own per-step error. (st, ct) are sin and cos of the
+// state's polar angle.
+template <typename R> __device__ __forceinline__ void k_project(KLane<R>& l) {
+    const KConst<R>& k = l.k;
+    const R r = l.s.r;
+    const R delta = fmaT(r, r - R(2), k.a2);
+    R inv_sin2, inv_sc;
+    k_sin_inverses(l.st, &inv_sin2, &inv_sc);
+    const R p = fmaT(r * r + k.a2, k.E, -k.aL);
+    const R g = fmaT(k.a2E2, k_sin2(l.st), fmaT(k.L2, inv_sin2, -k.two_aEL));
+    const R rest = p * p * rcp(delta) - l.s.pt * l.s.pt - g;  // Delta p_r^2 on the null cone
+    const R F = fmaT(delta, l.s.pr * l.s.pr, -rest);
+    const R carter = fmaT(l.ct * l.ct, fmaT(k.L2, inv_sin2, -k.a2E2), l.s.pt * l.s.pt);
+    l.gauge = gmax(l.gauge, gmax(gabs(carter - l.carter0), gabs(F) * rcp(gmax(r * r, R(1)))));
+    if (delta > R(0) && rest > R(0)) {
+        const R pr = sqrt(rest * rcp(delta));
+        if (gabs(pr - gabs(l.s.pr)) <= R(kProjectLimit) * gabs(l.s.pr)) {
+            l.s.pr = l.s.pr < R(0) ? -pr : pr;
+            l.c.pr = R(0);
+        }
+    }
+}
+
 // One iteration of marchRayKerr's loop (march.metal:140-173). The drift of
 // the state it starts from is folded in by k_increment (k_drift adds the
-// final state's).
-template <typename R, bool Comp = true>
+// final state's). Project: renormalise the state after each step
+// (k_project).
+template <typename R, bool Comp = true, bool Project = false>
 __device__ __forceinline__ bool k_step(KLane<R>& l, const MarchUniforms& u, cudaTextureObject_t em,
                                        cudaTextureObject_t vel, bool gather) {
     const GeodesicSettings& g = u.geodesic;
@@ -617,6 +702,7 @@ __device__ __forceinline__ bool k_step(KLane<R>& l, const MarchUniforms& u, cuda
     comp_addT<Comp>(l.s.pt, l.c.pt, inc.pt);
     l.steps += 1u;
     fast_sincos(l.s.th, &l.st, &l.ct);
+    if constexpr (Project) k_project(l);
     R sp, cp;
     V3<R> position = k_position(l, &sp, &cp);
     V3<R> d = position - l.previous;
@@ -695,9 +781,9 @@ template <typename R> __device__ inline RayProbeResult k_probe_result(const KLan
     return out;
 }
 
-// One pixel through the lane path, run to completion: compensated FP32, or
-// the FP64 re-integration with R = double.
-template <typename R, bool Comp = true>
+// One pixel through the lane path, run to completion: compensated FP32
+// (renormalised with Project), or the FP64 re-integration with R = double.
+template <typename R, bool Comp = true, bool Project = false>
 __device__ inline PixelResult shade_pixel_lane(const MarchParams& p, uint32_t px, uint32_t py) {
     const MarchUniforms& u = p.u;
     const bool gather = p.emission != 0;
@@ -707,19 +793,25 @@ __device__ inline PixelResult shade_pixel_lane(const MarchParams& p, uint32_t px
         KLane<R> l;
         k_init(l, origin, dir, u);
         for (uint32_t k = 0; k <= STEP_CAP_STILL; ++k)
-            if (k_step<R, Comp>(l, u, p.emission, p.velocity, gather)) break;
+            if (k_step<R, Comp, Project>(l, u, p.emission, p.velocity, gather)) break;
         return k_finish(l, u, p.blackbody);
     }
     SLane<R> l;
     float3 sky;
     if (s_init(l, origin, dir, u, p.tables, &sky)) return sky_only_result(sky, u, p.blackbody);
     for (uint32_t k = 0; k <= STEP_CAP_STILL; ++k)
-        if (s_step<R, Comp>(l, u, p.emission, p.velocity, gather)) break;
+        if (s_step<R, Comp, Project>(l, u, p.emission, p.velocity, gather)) break;
     return s_finish(l, u, p.tables, p.blackbody);
 }
 
 __device__ inline PixelResult shade_pixel_compensated(const MarchParams& p, uint32_t px, uint32_t py) {
     return shade_pixel_lane<float, true>(p, px, py);
+}
+
+// Compensated FP32 with the Hamiltonian-constraint renormalisation after
+// every step.
+__device__ inline PixelResult shade_pixel_renormalised(const MarchParams& p, uint32_t px, uint32_t py) {
+    return shade_pixel_lane<float, true, true>(p, px, py);
 }
 
 // The plain FP32 march: the same lane code with direct adds.

@@ -12,10 +12,10 @@
 
 namespace gg {
 
-// Mode: GG_PRECISION_PLAIN, _COMPENSATED or _PLAIN_AS_WRITTEN.
+// Mode: GG_PRECISION_PLAIN, _COMPENSATED, _PLAIN_AS_WRITTEN or _RENORMALISED.
 template <int Mode>
 __global__ void __launch_bounds__(256) march_image_kernel(MarchParams p) {
-    constexpr bool Comp = Mode == GG_PRECISION_COMPENSATED;
+    constexpr bool Comp = Mode == GG_PRECISION_COMPENSATED || Mode == GG_PRECISION_RENORMALISED;
     const uint32_t gx = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t gy = blockIdx.y * blockDim.y + threadIdx.y;
     const uint32_t px = p.u.tileOrigin.x + gx, py = p.u.tileOrigin.y + gy;
@@ -25,6 +25,7 @@ __global__ void __launch_bounds__(256) march_image_kernel(MarchParams p) {
     r.outcome = RayEscaped;
     if (active) {
         if constexpr (Mode == GG_PRECISION_COMPENSATED) r = shade_pixel_compensated(p, px, py);
+        else if constexpr (Mode == GG_PRECISION_RENORMALISED) r = shade_pixel_renormalised(p, px, py);
         else if constexpr (Mode == GG_PRECISION_PLAIN) r = shade_pixel_plain(p, px, py);
         else r = shade_pixel<float, false>(p, px, py);
         const uint32_t local = gy * p.target_width + gx;
@@ -119,9 +120,9 @@ __device__ RayProbeResult probe_one(const MarchParams& p, const RayProbe& q, flo
     return out;
 }
 
-// One probe through the lane code (the image kernels' arithmetic): plain or
-// compensated FP32, or FP64.
-template <typename R, bool Comp>
+// One probe through the lane code (the image kernels' arithmetic): plain,
+// compensated or renormalised FP32, or FP64.
+template <typename R, bool Comp, bool Project = false>
 __device__ RayProbeResult probe_lane(const MarchParams& p, const RayProbe& q, float* min_r) {
     const MarchUniforms& u = p.u;
     float3 origin = make_float3(q.origin.x, q.origin.y, q.origin.z);
@@ -130,7 +131,7 @@ __device__ RayProbeResult probe_lane(const MarchParams& p, const RayProbe& q, fl
         KLane<R> l;
         k_init(l, origin, dir, u);
         for (uint32_t k = 0; k <= STEP_CAP_STILL; ++k)
-            if (k_step<R, Comp>(l, u, 0, 0, false)) break;
+            if (k_step<R, Comp, Project>(l, u, 0, 0, false)) break;
         *min_r = l.min_r;
         return k_probe_result(l);
     }
@@ -139,7 +140,7 @@ __device__ RayProbeResult probe_lane(const MarchParams& p, const RayProbe& q, fl
     if (s_init(l, origin, dir, u, p.tables, &sky))
         return probe_one<float, false>(p, q, min_r);  // sky-only: no integration either way
     for (uint32_t k = 0; k <= STEP_CAP_STILL; ++k)
-        if (s_step<R, Comp>(l, u, 0, 0, false)) break;
+        if (s_step<R, Comp, Project>(l, u, 0, 0, false)) break;
     *min_r = l.min_r;
     return s_probe_result(l, u, p.tables);
 }
@@ -147,7 +148,8 @@ __device__ RayProbeResult probe_lane(const MarchParams& p, const RayProbe& q, fl
 template <int Mode>
 __global__ void __launch_bounds__(64) probe_kernel(MarchParams p, const RayProbe* __restrict__ probes,
                                                    RayProbeResult* __restrict__ results, uint32_t count) {
-    constexpr bool Comp = Mode == GG_PRECISION_COMPENSATED;
+    constexpr bool Comp = Mode == GG_PRECISION_COMPENSATED || Mode == GG_PRECISION_RENORMALISED;
+    constexpr bool Project = Mode == GG_PRECISION_RENORMALISED;
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= count) return;
     RayProbe q = probes[i];
@@ -156,7 +158,7 @@ __global__ void __launch_bounds__(64) probe_kernel(MarchParams p, const RayProbe
     if constexpr (Mode == GG_PRECISION_PLAIN_AS_WRITTEN) {
         r = probe_one<float, false>(p, q, &min_r);
     } else {
-        r = probe_lane<float, Comp>(p, q, &min_r);
+        r = probe_lane<float, Comp, Project>(p, q, &min_r);
         PixelResult pr{};
         pr.drift = r.drift;
         pr.min_r = min_r;
@@ -239,7 +241,7 @@ int launch_plain_image(const MarchParams& p, cudaStream_t stream, bool as_writte
 
 static bool known_precision(int precision) {
     return precision == GG_PRECISION_PLAIN || precision == GG_PRECISION_COMPENSATED ||
-           precision == GG_PRECISION_PLAIN_AS_WRITTEN;
+           precision == GG_PRECISION_PLAIN_AS_WRITTEN || precision == GG_PRECISION_RENORMALISED;
 }
 
 // The tables the uniforms enable must exist: sphereRadius > 0 means the
@@ -372,7 +374,7 @@ GG_API int gg_march(gg_context* ctx, const gg_volume* vol, const MarchUniforms* 
     p.stats = ctx->stats;
     GG_CUDA(cudaMemsetAsync(ctx->counters, 0, sizeof(MarchCounters), ctx->stream), "counter reset");
     GG_CUDA(cudaMemsetAsync(ctx->stats, 0, 4 * sizeof(unsigned long long), ctx->stream), "stats reset");
-    const bool comp = precision == GG_PRECISION_COMPENSATED;
+    const bool comp = precision == GG_PRECISION_COMPENSATED || precision == GG_PRECISION_RENORMALISED;
     if (comp) {
         // Scratch: the flagged-pixel list (one entry per target pixel at most)
         // and its counter, in one buffer.
@@ -387,7 +389,10 @@ GG_API int gg_march(gg_context* ctx, const gg_volume* vol, const MarchUniforms* 
     dim3 block(p.block_w, p.block_h);
     dim3 grid((targets->width + block.x - 1) / block.x, (targets->height + block.y - 1) / block.y);
     if (comp) {
-        march_image_kernel<GG_PRECISION_COMPENSATED><<<grid, block, 0, ctx->stream>>>(p);
+        if (precision == GG_PRECISION_RENORMALISED)
+            march_image_kernel<GG_PRECISION_RENORMALISED><<<grid, block, 0, ctx->stream>>>(p);
+        else
+            march_image_kernel<GG_PRECISION_COMPENSATED><<<grid, block, 0, ctx->stream>>>(p);
         GG_CHECK(gg::launch_status("march"));
         reintegrate_kernel<<<ctx->sm_count, 128, 0, ctx->stream>>>(p);
     } else if (precision == GG_PRECISION_PLAIN) {
@@ -502,6 +507,8 @@ GG_API int gg_probe(gg_context* ctx, const MarchUniforms* u, const RayProbe* pro
     const unsigned blocks = (count + 63u) / 64u;
     if (precision == GG_PRECISION_COMPENSATED)
         probe_kernel<GG_PRECISION_COMPENSATED><<<blocks, 64, 0, ctx->stream>>>(p, d_in, d_out, count);
+    else if (precision == GG_PRECISION_RENORMALISED)
+        probe_kernel<GG_PRECISION_RENORMALISED><<<blocks, 64, 0, ctx->stream>>>(p, d_in, d_out, count);
     else if (precision == GG_PRECISION_PLAIN)
         probe_kernel<GG_PRECISION_PLAIN><<<blocks, 64, 0, ctx->stream>>>(p, d_in, d_out, count);
     else

@@ -181,4 +181,4 @@ LAYOUT = {
 
 RAY_CAPTURED, RAY_ESCAPED, RAY_EXHAUSTED = 0, 1, 2
 POTENTIAL_NEWTONIAN, POTENTIAL_PACZYNSKI_WIITA = 0, 1
-PRECISION_PLAIN, PRECISION_COMPENSATED, PRECISION_PLAIN_AS_WRITTEN = 0, 1, 2
+PRECISION_PLAIN, PRECISION_COMPENSATED, PRECISION_PLAIN_AS_WRITTEN, PRECISION_RENORMALISED = 0, 1, 2, 3

@@ -256,7 +256,16 @@ typedef enum {
     /* FP32 with the reference kernel's arithmetic as written: four
      * derivative calls per step with their divides, library sin/cos
      * (Geodesic.h:42-59, Kerr.h:63-99). The per-request baseline. */
-    GG_PRECISION_PLAIN_AS_WRITTEN = 2
+    GG_PRECISION_PLAIN_AS_WRITTEN = 2,
+    /* GG_PRECISION_COMPENSATED with the Hamiltonian-constraint
+     * renormalisation after every step: a Schwarzschild state is put back on
+     * the null cone with its starting E and L (phiDot from L, rDot and vDot
+     * from E and the constraint, in double); a Kerr state gets |p_r| from
+     * 2 Sigma H = 0 (Kerr.h:39-50). The drift reported is the largest drift
+     * of a state before its projection, the integrator's per-step error
+     * (after it the gauges read roundoff by construction). gg_march and
+     * gg_probe; no reference counterpart. */
+    GG_PRECISION_RENORMALISED = 3
 } gg_precision;
 
 /* Which flagged rays the compensated march re-integrates in FP64. A ray is

@@ -261,24 +261,28 @@ def test_shadow_kerr(world):
 # kernel runs (gg_probe with GG_PRECISION_COMPENSATED shares its lane code).
 
 COMP = 1
+RENORM = 3  # compensated with the Hamiltonian-constraint renormalisation
+BOTH = pytest.mark.parametrize("prec", [COMP, RENORM], ids=["compensated", "renormalised"])
 
 
-def test_conservation_still_compensated(world):
+@BOTH
+def test_conservation_still_compensated(world, prec):
     import gargantua_b200 as g
 
     golden = load_golden("conservation_still")
     launches = g.camera_grid(g.OrbitCamera(), 16, 16, 960 / 540)
-    res = world["ctx"].probe(launches, probe_uniforms(g, world["ctx"], g.Settings.still()), COMP)
+    res = world["ctx"].probe(launches, probe_uniforms(g, world["ctx"], g.Settings.still()), prec)
     worst = float(res["drift"].max())
     assert golden_passes(golden, worst), f"max drift {worst:.2e}"
 
 
-def test_parity_compensated(world):
+@BOTH
+def test_parity_compensated(world, prec):
     import gargantua_b200 as g
 
     golden = load_golden("parity")
     launches = [g.as_float32_launch(l) for l in g.camera_grid(g.OrbitCamera(), 8, 8, 960 / 540)]
-    gpu = world["ctx"].probe(launches, probe_uniforms(g, world["ctx"], g.Settings.still()), COMP)
+    gpu = world["ctx"].probe(launches, probe_uniforms(g, world["ctx"], g.Settings.still()), prec)
     probes = np.array([np.concatenate([l.origin, l.direction]) for l in launches])
     ref = O.integrate_batch(probes, O.still(), THREADS)
     dist = np.linalg.norm(ref[:, :3] - gpu["position"].astype(np.float64), axis=1) / np.maximum(
@@ -287,12 +291,13 @@ def test_parity_compensated(world):
     assert golden_passes(golden, float(dist.max())) and mismatches == 0, (float(dist.max()), mismatches)
 
 
-def test_sky_compensated(world):
+@BOTH
+def test_sky_compensated(world, prec):
     import gargantua_b200 as g
 
     golden = load_golden("sky")
     launches = [g.as_float32_launch(l) for l in g.camera_grid(g.OrbitCamera(), 8, 8, 960 / 540)]
-    gpu = world["ctx"].probe(launches, probe_uniforms(g, world["ctx"], g.Settings.still(), jump=True), COMP)
+    gpu = world["ctx"].probe(launches, probe_uniforms(g, world["ctx"], g.Settings.still(), jump=True), prec)
     st = O.Settings(0.01, 0.02, 20.0, 2.02, 1e6, 400_000, 0.02, 20.0)
     probes = np.array([np.concatenate([l.origin, l.direction]) for l in launches])
     ref = O.integrate_batch(probes, st, THREADS)
@@ -306,7 +311,8 @@ def test_sky_compensated(world):
     assert golden_passes(golden, worst) and mism == 0, (worst, mism)
 
 
-def test_shadow_kerr_compensated(world):
+@BOTH
+def test_shadow_kerr_compensated(world, prec):
     import ctypes as C
 
     import gargantua_b200 as g
@@ -320,7 +326,7 @@ def test_shadow_kerr_compensated(world):
         for _ in range(iterations):
             aim = 0.5 * (low + high)
             res = world["ctx"].probe([g.Launch(np.array([radius, 0.0, 0.0]), np.array([-1.0, side * aim, 0.0]))], u,
-                                     COMP)
+                                     prec)
             low, high = (aim, high) if res["outcome"][0] == 0 else (low, aim)
         s = np.zeros(7)
         O.lib().o_kerr_launch(spin, np.array([radius, 0.0, 0.0]), np.array([-1.0, side * 0.5 * (low + high), 0.0]), s)
@@ -342,7 +348,7 @@ def test_kerr_probe_parity_against_fp64_oracle(world):
     launches = [g.as_float32_launch(l) for l in g.camera_grid(cam, 8, 8, 16 / 9)]
     probes = np.array([np.concatenate([l.origin, l.direction]) for l in launches])
     ref = O.kerr_integrate_batch(0.9, probes, O.kerr_settings(4096), THREADS)
-    for prec in (0, COMP):
+    for prec in (0, COMP, RENORM):
         gpu = world["ctx"].probe(launches, probe_uniforms(g, world["ctx"], g.Settings.still(), spin=0.9), prec)
         same = ref[:, 7].astype(int) == gpu["outcome"].astype(int)
         assert same.mean() >= 0.95, same.mean()
