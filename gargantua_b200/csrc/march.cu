@@ -305,6 +305,7 @@ GG_API void gg_targets_destroy(gg_targets* t) {
     gg::device_free(ctx, t->debug, px * 8u);
     gg::device_free(ctx, t->depth, px * 4u);
     gg::device_free(ctx, t->motion, px * 4u);
+    if (t->srgb) gg::device_free(ctx, t->srgb, px * 4u);
     delete t;
 }
 

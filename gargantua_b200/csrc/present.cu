@@ -118,16 +118,15 @@ GG_API int gg_tonemap(gg_targets* t, const PresentUniforms* u, uint8_t* rgba8) {
     std::lock_guard<std::recursive_mutex> lock(ctx->mu);
     GG_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
     const uint32_t count = t->width * t->height;
-    uchar4* d_out = nullptr;
-    GG_CHECK(gg::device_alloc(ctx, (uint64_t)count * 4u, (void**)&d_out, "tone-mapped image"));
-    tonemap_kernel<<<(count + 255u) / 256u, 256, 0, ctx->stream>>>(t->color, t->debug, *u, count, d_out);
-    int s = gg::launch_status("tone map");
-    if (s == GG_OK)
-        s = gg::cuda_status(cudaMemcpyAsync(rgba8, d_out, (size_t)count * 4u, cudaMemcpyDeviceToHost, ctx->stream),
-                            "tone map readback");
-    if (s == GG_OK) s = gg::cuda_status(cudaStreamSynchronize(ctx->stream), "tone map");
-    gg::device_free(ctx, d_out, (uint64_t)count * 4u);
-    return s;
+    // The 8-bit image's device buffer stays with the targets (freed with
+    // them), so a frame loop's tone maps allocate nothing after the first.
+    if (!t->srgb) GG_CHECK(gg::device_alloc(ctx, (uint64_t)count * 4u, (void**)&t->srgb, "tone-mapped image"));
+    tonemap_kernel<<<(count + 255u) / 256u, 256, 0, ctx->stream>>>(t->color, t->debug, *u, count, t->srgb);
+    GG_CHECK(gg::launch_status("tone map"));
+    GG_CUDA(cudaMemcpyAsync(rgba8, t->srgb, (size_t)count * 4u, cudaMemcpyDeviceToHost, ctx->stream),
+            "tone map readback");
+    GG_CUDA(cudaStreamSynchronize(ctx->stream), "tone map");
+    return GG_OK;
 }
 
 GG_API int gg_write_png(const char* path, const uint8_t* rgba8, uint32_t width, uint32_t height) {

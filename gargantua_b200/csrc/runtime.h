@@ -150,6 +150,7 @@ struct gg_targets {
     float* depth = nullptr;
     ushort2* motion = nullptr;
     uint64_t bytes = 0;
+    uchar4* srgb = nullptr;  // gg_tonemap's device output, allocated by its first call and kept
 };
 
 struct gg_bake {

@@ -48,6 +48,16 @@ __device__ __forceinline__ float len3(float x, float y, float z) { return sqrtf(
 // sqrt(s) < 2.02f exactly when s < 4.0803995f (bits 0x408292a2, the least
 // float whose square root rounds to 2.02f or above). Both bounds were found
 // by testing every float near the squares; a CPU test repeats that search.
+// g(r) = 1 / kick_denominator(r): d^2 with d = max(r - 2, 1e-6) for
+// Paczynski-Wiita, r^2 for Newton (Common.h:32-46).
+__device__ __forceinline__ float kick_denominator(float r, uint32_t potential) {
+    if (potential == PotentialPaczynskiWiita) {
+        float d = fmaxf(r - R_SCHWARZSCHILD, 1e-6f);
+        return d * d;
+    }
+    return r * r;
+}
+
 constexpr float kPlungeSpeedSquared = 144.0f;
 constexpr uint32_t kCaptureClosestSquaredBits = 0x408292a2u;
 static_assert(PLUNGE_SPEED_LIMIT == 12.0f && R_CAPTURE == 2.02f, "the squared bounds belong to these limits");
@@ -116,10 +126,12 @@ __global__ void __launch_bounds__(256) seed_kernel(SimArgs a) {
 // R_ESCAPE or outruns PLUNGE_SPEED_LIMIT; the temperature follows the final
 // radius.
 //
-// Two changes against the reference's arithmetic, shared with the CPU
-// replica: the angular frequency is sqrt(-k) = sqrt(g / r), where the
-// reference divides circular_speed(r) = sqrt(r g) by r (the same quantity,
-// one divide fewer); and the chord's closest approach is only computed when
+// Three changes against the reference's arithmetic, shared with the CPU
+// replica: the kick factor k = -g(r) / r is one divide, -1 / (d^2 r) with d
+// = max(r - 2, 1e-6) (the reference divides 1 / d^2 by r); the angular
+// frequency is sqrt(-k) = sqrt(g / r), where the reference divides
+// circular_speed(r) = sqrt(r g) by r (the same quantity, one divide fewer);
+// and the chord's closest approach is only computed when
 // it can matter. A substep that starts at |x| > 4 and moves less than 1
 // keeps every point of its chord more than 3 from the centre, so the
 // computed squared distance (exact up to a few ulps) is far above the
@@ -137,7 +149,7 @@ __global__ void __launch_bounds__(256) step_kernel(SimArgs a) {
     float r = len3(px, py, pz);  // |x| at the start of each substep
 #pragma unroll
     for (uint32_t s = 0; s < SIM_SUBSTEPS; ++s) {
-        float k = -potential_gradient(r, u.potential) / r;
+        float k = -1.0f / (kick_denominator(r, u.potential) * r);
         float omega = sqrtf(-k);
         const float r_before = r;
         vx = vx + px * k * u.dt;

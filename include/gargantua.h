@@ -383,7 +383,9 @@ GG_API int gg_bake_read(gg_bake* b, uint16_t* samples_half4, BakedRay* headers);
  * encoding) into width*height*4 bytes of 8-bit sRGB RGBA on the host, or, with
  * u->debugView != 0, the drift heat map of the debug target. Replaces the
  * present pass's tonemapFragment (present.metal:22-58) with a headless
- * buffer in place of the drawable. */
+ * buffer in place of the drawable. The first call on a targets handle
+ * allocates its 4 bytes per pixel of device output, kept until
+ * gg_targets_destroy. */
 GG_API int gg_tonemap(gg_targets* t, const PresentUniforms* u, uint8_t* rgba8);
 
 /* Write an 8-bit RGBA image as a PNG file (zlib-compressed, no filter).

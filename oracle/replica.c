@@ -106,15 +106,25 @@ static void spawn32(uint32_t index, uint32_t event, const sim32* u, int from_dis
     memcpy(&p[7], &event, 4);
 }
 
-/* sim.metal:44-79, with the angular frequency as sqrt(-k) = sqrt(g / r)
- * (the reference divides circular_speed(r) = sqrt(r g) by r), as the
- * kernel computes it. */
+/* g(r) = 1 / kick_denominator(r) (Common.h:32-46). */
+static float kick_denominator(float r, uint32_t potential) {
+    if (potential == PotentialPaczynskiWiita) {
+        float d = fmaxf(r - R_SCHWARZSCHILD, 1e-6f);
+        return d * d;
+    }
+    return r * r;
+}
+
+/* sim.metal:44-79, with the kick factor as one divide, k = -1 / (d^2 r)
+ * (the reference divides 1 / d^2 by r), and the angular frequency as
+ * sqrt(-k) = sqrt(g / r) (the reference divides circular_speed(r) =
+ * sqrt(r g) by r), as the kernel computes them. */
 static void step32(uint32_t i, const sim32* u, float* p) {
     float px = p[0], py = p[1], pz = p[2];
     float vx = p[3], vy = p[4], vz = p[5];
     for (uint32_t s = 0; s < SIM_SUBSTEPS; ++s) {
         float r = length3f(px, py, pz);
-        float k = -gradf(r, u->potential) / r;
+        float k = -1.0f / (kick_denominator(r, u->potential) * r);
         float omega = sqrtf(-k);
         vx = vx + px * k * u->dt;
         vy = vy + py * k * u->dt;
