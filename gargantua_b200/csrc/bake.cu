@@ -28,6 +28,9 @@ struct BakeArgs {
     BakedRay* headers;
     uint32_t* overflow;
     uint32_t rows;
+    // Optional (NULL: not kept): [0] += RK4 steps, [5] += rays that ran out
+    // of steps, [6] += captured rays (a served request's counter words).
+    unsigned long long* stats;
 };
 
 // bakeRays (bake.metal:17-92).
@@ -46,6 +49,22 @@ __global__ void __launch_bounds__(64) bake_kernel(BakeArgs a) {
     float ny = (1.0f - 2.0f * sy / (float)u.resolution.y) * u.tanHalfFov.y;
     float3 dir = normalize3(to_f3(u.cameraForward) + nx * to_f3(u.cameraRight) + ny * to_f3(u.cameraUp));
     PreparedRay<float> prepared = prepare_ray(to_v3<float>(to_f3(u.cameraPosition)), to_v3<float>(dir), u, a.p.tables);
+    uint32_t steps = 0;
+    uint32_t outcome = RayEscaped;
+    // Per-warp sums of the served request's counters, taken by the threads
+    // still running (sky-only rays count as escaped with no steps).
+    auto count = [&] {
+        if (!a.stats) return;
+        const unsigned mask = __activemask();
+        const uint32_t s = __reduce_add_sync(mask, steps);
+        const uint32_t e = __reduce_add_sync(mask, outcome == RayExhausted ? 1u : 0u);
+        const uint32_t c = __reduce_add_sync(mask, outcome == RayCaptured ? 1u : 0u);
+        if ((uint32_t)(__ffs(mask) - 1) == (threadIdx.x + threadIdx.y * blockDim.x) % 32u) {
+            if (s) atomicAdd(&a.stats[0], (unsigned long long)s);
+            if (e) atomicAdd(&a.stats[5], (unsigned long long)e);
+            if (c) atomicAdd(&a.stats[6], (unsigned long long)c);
+        }
+    };
     if (prepared.skyOnly) {
         BakedRay h;
         h.count = 0u;
@@ -53,21 +72,23 @@ __global__ void __launch_bounds__(64) bake_kernel(BakeArgs a) {
         h.directionXY = pack_half2(prepared.sky.x, prepared.sky.y);
         h.directionZDepth = pack_half2(prepared.sky.z, 1.0f);
         a.headers[index] = h;
+        count();
         return;
     }
     PlaneRay<float> ray = prepared.ray;
     const GeodesicSettings& g = u.geodesic;
     V3<float> previous = ray_position(ray);
     float since = 0.0f, travelled = 0.0f, first_depth = -1.0f;
-    uint32_t count = 0;
+    uint32_t stored = 0;
     bool overflowed = false, left_sphere = false;
-    uint32_t outcome = RayExhausted;
+    outcome = RayExhausted;
     const float sphere = u.sphereRadius;
     for (uint32_t k = 0; k < STEP_CAP_STILL; ++k) {
         if (k >= g.stepCap) break;
         float h = ray_step_length(previous.z, ray.s.r, g);
         RayState<float> before = ray.s;
         ray.s = ray_step(ray.s, h);
+        steps += 1u;
         if (sphere > 0.0f && ray.s.r >= sphere && ray.s.rDot > 0.0f && before.r < sphere)
             ray.s = ray_step(before, h * (sphere - before.r) / (ray.s.r - before.r));
         V3<float> position = ray_position(ray);
@@ -81,9 +102,9 @@ __global__ void __launch_bounds__(64) bake_kernel(BakeArgs a) {
         }
         float3 pf = to_float3(position);
         if (in_slab(pf, u.volumeHalfExtent) && since >= u.bakeSpacing) {
-            if (count < u.bakeCapacity) {
-                slot[count] = pack_half4(pf.x, pf.y, pf.z, since);
-                count += 1u;
+            if (stored < u.bakeCapacity) {
+                slot[stored] = pack_half4(pf.x, pf.y, pf.z, since);
+                stored += 1u;
                 if (first_depth < 0.0f) first_depth = travelled;
             } else {
                 overflowed = true;
@@ -104,12 +125,13 @@ __global__ void __launch_bounds__(64) bake_kernel(BakeArgs a) {
     V3<float> fin = left_sphere ? sphere_exit_direction(ray, u, a.p.tables) : ray_direction(ray);
     float depth = first_depth >= 0.0f ? first_depth : travelled;
     BakedRay hd;
-    hd.count = count;
+    hd.count = stored;
     hd.fallsIn = falls_in ? 1u : 0u;
     hd.directionXY = pack_half2(fin.x, fin.y);
     hd.directionZDepth = pack_half2(fin.z, fminf(depth / (2.0f * R_ESCAPE), 1.0f));
     a.headers[index] = hd;
     if (overflowed) atomicAdd(a.overflow, 1u);
+    count();
 }
 
 struct WalkArgs {
@@ -175,6 +197,33 @@ __global__ void __launch_bounds__(64) walk_kernel(WalkArgs a) {
 
 MarchParams make_params(gg_context* ctx, const gg_volume* vol, const MarchUniforms& u, const gg_sweep* sweep);
 int check_uniforms(gg_context* ctx, const MarchUniforms* u, const char* what);
+
+// A served bake request (the server's GG_REQUEST_BAKE): every row baked with
+// `bake` (its tables, spacing and capacity set), then walked through
+// `walk`'s volume into walk.color, on `stream`. stats: the request's
+// counter words (see BakeArgs), or NULL.
+int launch_bake_walk(const MarchParams& bake, const MarchParams& walk, ushort4* samples, BakedRay* headers,
+                     uint32_t* overflow, unsigned long long* stats, cudaStream_t stream) {
+    BakeArgs b{};
+    b.p = bake;
+    b.p.u.tileOrigin.x = 0;
+    b.p.u.tileOrigin.y = 0;
+    b.samples = samples;
+    b.headers = headers;
+    b.overflow = overflow;
+    b.rows = bake.u.resolution.y;
+    b.stats = stats;
+    dim3 block(MARCH_THREADGROUP_WIDTH, MARCH_THREADGROUP_HEIGHT);
+    dim3 grid((bake.u.resolution.x + block.x - 1) / block.x, (b.rows + block.y - 1) / block.y);
+    bake_kernel<<<grid, block, 0, stream>>>(b);
+    GG_CHECK(launch_status("served bake"));
+    WalkArgs w{};
+    w.p = walk;
+    w.samples = samples;
+    w.headers = headers;
+    walk_kernel<<<grid, block, 0, stream>>>(w);
+    return launch_status("served walk");
+}
 
 }  // namespace gg
 

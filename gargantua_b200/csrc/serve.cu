@@ -44,6 +44,8 @@ namespace gg {
 
 MarchParams make_params(gg_context* ctx, const gg_volume* vol, const MarchUniforms& u, const gg_sweep* sweep);
 int launch_plain_image(const MarchParams& p, cudaStream_t stream, bool as_written);
+int launch_bake_walk(const MarchParams& bake, const MarchParams& walk, ushort4* samples, BakedRay* headers,
+                     uint32_t* overflow, unsigned long long* stats, cudaStream_t stream);
 
 struct ServeRequest {
     MarchUniforms u;
@@ -391,6 +393,13 @@ struct ServedRequest {
     gg_sweep sweep;
     ushort4* d_color = nullptr;
     ushort4* d_debug = nullptr;
+    // GG_REQUEST_BAKE: the bake storage (BakePass.swift:31-38), its
+    // overflow count, and whether the bake and walk were launched.
+    bool bake = false;
+    ushort4* d_samples = nullptr;
+    BakedRay* d_headers = nullptr;
+    uint32_t* d_overflow = nullptr;
+    cudaEvent_t baked = nullptr;
     unsigned long long* d_stats = nullptr;  // 8 u64 then a MarchCounters
     uint64_t footprint = 0;
     uint32_t rays = 0;
@@ -504,6 +513,15 @@ static int admit(gg_server* s, const std::shared_ptr<ServedRequest>& r) {
         GG_CUDA(cudaMallocFromPoolAsync((void**)&r->d_debug, px * 8u, s->pool, s->build), "request debug target");
     GG_CUDA(cudaMallocFromPoolAsync((void**)&r->d_stats, 128, s->pool, s->build), "request counters");
     GG_CUDA(cudaMemsetAsync(r->d_stats, 0, 128, s->build), "request counters");
+    if (r->bake) {
+        GG_CUDA(cudaMallocFromPoolAsync((void**)&r->d_samples, px * BAKE_SAMPLES * 8u, s->pool, s->build),
+                "request bake samples");
+        GG_CUDA(cudaMallocFromPoolAsync((void**)&r->d_headers, px * 16u, s->pool, s->build), "request bake headers");
+        GG_CUDA(cudaMallocFromPoolAsync((void**)&r->d_overflow, 4u, s->pool, s->build), "request bake overflow");
+        GG_CUDA(cudaMemsetAsync(r->d_overflow, 0, 4u, s->build), "request bake overflow");
+        // The walk writes colour only: the debug target, if asked for, stays zero.
+        if (r->d_debug) GG_CUDA(cudaMemsetAsync(r->d_debug, 0, px * 8u, s->build), "request debug target");
+    }
     if (r->q.spin == 0.0f) {
         GG_CUDA(cudaMallocFromPoolAsync((void**)&r->sweep.camera, SWEEP_TABLE_SIZE * sizeof(float), s->pool, s->build),
                 "camera table");
@@ -518,6 +536,16 @@ static int admit(gg_server* s, const std::shared_ptr<ServedRequest>& r) {
 }
 
 static void release(gg_server* s, ServedRequest& r) {
+    if (r.bake) {
+        cudaFreeAsync(r.d_samples, s->copy);
+        cudaFreeAsync(r.d_headers, s->copy);
+        cudaFreeAsync(r.d_overflow, s->copy);
+        r.d_samples = nullptr;
+        r.d_headers = nullptr;
+        r.d_overflow = nullptr;
+        if (r.baked) cudaEventDestroy(r.baked);
+        r.baked = nullptr;
+    }
     cudaFreeAsync(r.d_color, s->copy);
     if (r.d_debug) cudaFreeAsync(r.d_debug, s->copy);
     cudaFreeAsync(r.d_stats, s->copy);
@@ -542,6 +570,28 @@ static int start_copy(gg_server* s, ServedRequest& r, cudaEvent_t after) {
     GG_CUDA(cudaEventCreateWithFlags(&r.copied, cudaEventDisableTiming), "copy event");
     GG_CUDA(cudaEventRecord(r.copied, s->copy), "copy event");
     r.copying = true;
+    return GG_OK;
+}
+
+// A GG_REQUEST_BAKE request: the bake of every row at the request's step
+// policy and BakePass.spacing (BakePass.swift:50-52) for its volume's size,
+// then the walk through that volume into its colour target, on `stream`
+// after the tables are built; its copy follows. Its rays join no wave.
+static int launch_bake(gg_server* s, ServedRequest& r, cudaStream_t stream, cudaEvent_t* done) {
+    gg_context* ctx = s->ctx;
+    const gg_volume* vol = request_volume(s, r);
+    GG_CUDA(cudaStreamWaitEvent(stream, s->built, 0), "bake ordering");
+    MarchUniforms ub = r.u;
+    ub.bakeSpacing = (float)(2.0 * VOLUME_HALF_EXTENT / (double)(vol ? vol->size : 128u) * BAKE_SPACING_VOXELS);
+    ub.bakeCapacity = BAKE_SAMPLES;
+    MarchParams pb = make_params(ctx, nullptr, ub, &r.sweep);
+    MarchParams pw = make_params(ctx, vol, ub, nullptr);
+    pw.color = r.d_color;
+    GG_CHECK(launch_bake_walk(pb, pw, r.d_samples, r.d_headers, r.d_overflow, r.d_stats, stream));
+    GG_CUDA(cudaEventCreateWithFlags(&r.baked, cudaEventDisableTiming), "bake event");
+    GG_CUDA(cudaEventRecord(r.baked, stream), "bake event");
+    r.next_ray = r.rays;
+    *done = r.baked;
     return GG_OK;
 }
 
@@ -654,6 +704,19 @@ static int finish_wave(gg_server* s, WaveSlot& w) {
 // caller records it (and the launch count) once it holds the mutex again.
 static int run_plain(gg_server* s, ServedRequest& r, std::pair<double, double>* interval) {
     gg_context* ctx = s->ctx;
+    if (r.bake) {
+        GG_CUDA(cudaEventRecord(s->slots[0].start, s->plain), "plain event");
+        cudaEvent_t done = nullptr;
+        GG_CHECK(launch_bake(s, r, s->plain, &done));
+        GG_CUDA(cudaEventRecord(s->slots[0].stop, s->plain), "plain event");
+        GG_CHECK(start_copy(s, r, s->slots[0].stop));
+        GG_CUDA(cudaEventSynchronize(r.copied), "plain bake");
+        float t0 = 0.0f, t1 = 0.0f;
+        GG_CUDA(cudaEventElapsedTime(&t0, s->origin, s->slots[0].start), "plain timing");
+        GG_CUDA(cudaEventElapsedTime(&t1, s->origin, s->slots[0].stop), "plain timing");
+        *interval = std::make_pair((double)t0 * 1e-3, (double)t1 * 1e-3);
+        return GG_OK;
+    }
     GG_CUDA(cudaStreamWaitEvent(s->plain, s->built, 0), "plain ordering");
     MarchParams p = make_params(ctx, request_volume(s, r), r.u, r.q.spin == 0.0f ? &r.sweep : nullptr);
     p.color = r.d_color;
@@ -681,8 +744,12 @@ static void complete_request(gg_server* s, ServedRequest& r) {
     r.result.ray_steps = r.host_stats[0];
     r.result.samples = r.host_stats[1];
     r.result.fp64_rays = r.host_stats[2];
-    if (serial(s)) {
+    if (serial(s) && !r.bake) {
         std::memcpy(&r.result.counters, &r.host_stats[8], sizeof(MarchCounters));
+    } else if (r.bake) {
+        r.result.counters.rays = r.rays;
+        r.result.counters.exhausted = (uint32_t)r.host_stats[5];
+        r.result.counters.captured = (uint32_t)r.host_stats[6];
     } else {
         r.result.counters.rays = (uint32_t)r.host_stats[3];
         r.result.counters.overDriftBudget = (uint32_t)r.host_stats[4];
@@ -734,6 +801,14 @@ static void worker_loop(gg_server* s) {
                         }
                     }
             } else {
+                // Bake requests run beside the waves on their own stream.
+                for (auto& r : s->admitted) {
+                    if (!r->bake || r->baked || status != GG_OK) continue;
+                    cudaEvent_t done = nullptr;
+                    status = launch_bake(s, *r, s->plain, &done);
+                    if (status == GG_OK) status = start_copy(s, *r, done);
+                    if (status == GG_OK) s->total_launches += 2;
+                }
                 for (uint32_t k = 0; k < s->slots.size() && status == GG_OK; ++k) {
                     WaveSlot& w = s->slots[(s->next_slot + k) % s->slots.size()];
                     if (w.busy) continue;
@@ -969,11 +1044,16 @@ GG_API int gg_server_submit(gg_server* s, const gg_request* req, uint64_t* ticke
     if (!req->output) return gg::fail(GG_ERR_INVALID_ARGUMENT, "The request has no output buffer.");
     if (req->volume && req->volume->ctx != s->ctx)
         return gg::fail(GG_ERR_INVALID_ARGUMENT, "The request's volume belongs to another context.");
+    const bool bake = (req->flags & GG_REQUEST_BAKE) != 0u;
+    if (bake && req->spin != 0.0f)
+        return gg::fail(GG_ERR_UNSUPPORTED, "The bake strategy is Schwarzschild only; spin %g was given.", (double)req->spin);
     auto r = std::make_shared<gg::ServedRequest>();
     r->q = *req;
     r->u = gg::request_uniforms(*req);
     r->rays = req->width * req->height;
+    r->bake = bake;
     r->footprint = (uint64_t)r->rays * (req->debug_output ? 16u : 8u) + 128u + 2u * SWEEP_TABLE_SIZE * 4u;
+    if (bake) r->footprint += (uint64_t)r->rays * (BAKE_SAMPLES * 8u + 16u) + 4u;
     std::lock_guard<std::mutex> lock(s->mu);
     if (s->fatal != GG_OK) return gg::fail(s->fatal, "The server stopped after a device error: %s", s->fatal_sentence.c_str());
     if (r->footprint > s->cfg.memory_bytes)

@@ -162,7 +162,7 @@ SCHEDULE_CHUNKS, SCHEDULE_LANE_REFILL = 0, 1
 
 FP64_ESCAPING, FP64_ALL_FLAGGED = 0, 1
 SERVE_BATCHED, SERVE_SERIAL_PLAIN, SERVE_SERIAL_PLAIN_AS_WRITTEN = 0, 1, 2
-REQUEST_NO_STARS, REQUEST_NO_REDSHIFT = 1, 2
+REQUEST_NO_STARS, REQUEST_NO_REDSHIFT, REQUEST_BAKE = 1, 2, 4
 
 
 # Sizes the C header pins with static assertions (gargantua_types.h).

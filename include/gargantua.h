@@ -421,6 +421,13 @@ typedef struct {
 
 #define GG_REQUEST_NO_STARS 1u   /* starBrightness 0 */
 #define GG_REQUEST_NO_REDSHIFT 2u
+/* The bake strategy (bake.metal:17-144, BakePass.swift): the request's rays
+ * are integrated once at its step policy with their in-slab points stored
+ * (BAKE_SAMPLES half4 and a 16-byte header per pixel, about 400 MB at
+ * 960x540, counted in the request's admission footprint), then walked
+ * through its volume into the output; the debug output stays zero.
+ * Schwarzschild only (GG_ERR_UNSUPPORTED for spin > 0). */
+#define GG_REQUEST_BAKE 4u
 
 /* Per-request outcome, times in seconds on the server's monotonic clock. */
 typedef struct {

@@ -243,3 +243,54 @@ def test_schedules_give_the_same_pixels(world):
         assert np.abs(pa.astype(np.float64) - pb.astype(np.float64)).max() < 1e-3
         la, lb = luminance(pa), luminance(pb)
         assert np.abs(la - lb).sum() / max(lb.sum(), 1e-30) < 1e-5
+
+
+def test_bake_requests_are_served_beside_marches(world):
+    """GG_REQUEST_BAKE (the bake strategy as a served request): the walk of
+    its bake renders the march's image of the same camera (image light
+    within 1 %, the jump golden's bar for two quadratures of one image), it
+    reports its ray steps, and its pixels are the same alone, in a mix with
+    marches, and through the one-at-a-time baseline server."""
+    import gargantua_b200 as g
+
+    bake = g.RequestSpec(480, 270, 4096, 0.0, azimuth=0.9, elevation=0.3, distance=58.0, flags=g.types.REQUEST_BAKE)
+    march = g.RequestSpec(480, 270, 4096, 0.0, azimuth=0.9, elevation=0.3, distance=58.0)
+    server = g.Server(world["ctx"], world["vol"], g.types.SERVE_BATCHED)
+    mixed = run(server, [bake, march, g.RequestSpec(320, 180, 256, 0.9)], debug=True)
+    (bp, bd, br), (mp, _, mr) = mixed[0], mixed[1]
+    assert br.counters.rays == 480 * 270 and br.ray_steps > 0
+    assert not bd.any()  # the walk writes colour only
+    lb, lm = luminance(bp), luminance(mp)
+    assert abs(lb.sum() - lm.sum()) / lm.sum() < 0.01, abs(lb.sum() - lm.sum()) / lm.sum()
+    alone = run(server, [bake])[0]
+    assert np.array_equal(alone[0].view(np.uint16), bp.view(np.uint16))
+    assert alone[2].ray_steps == br.ray_steps
+    server.close()
+    serial = g.Server(world["ctx"], world["vol"], g.types.SERVE_SERIAL_PLAIN)
+    one = run(serial, [bake])[0]
+    assert np.array_equal(one[0].view(np.uint16), bp.view(np.uint16)) and one[2].ray_steps == br.ray_steps
+    serial.close()
+
+
+def test_bake_storage_counts_in_admission(world):
+    """A bake request's footprint holds its stored samples (96 half4 and a
+    16-byte header per pixel): with memory for one such request at a time,
+    three are served one after another, each admitted once the previous one
+    released its storage, all with the same pixels. A Kerr bake is
+    refused."""
+    import gargantua_b200 as g
+
+    spec = g.RequestSpec(480, 270, 256, 0.0, flags=g.types.REQUEST_BAKE)
+    one = 480 * 270 * (8 + 96 * 8 + 16) + 128 + 8192 + 4
+    server = g.Server(world["ctx"], world["vol"], g.types.SERVE_BATCHED, memory_bytes=int(one * 1.5))
+    results = run(server, [spec] * 3)
+    for pix, _, res in results:
+        assert res.counters.rays == 480 * 270
+        assert np.array_equal(pix.view(np.uint16), results[0][0].view(np.uint16))
+    order = sorted(results, key=lambda r: r[2].admitted)
+    for before, after in zip(order, order[1:]):
+        assert after[2].admitted >= before[2].finished  # admitted only once storage frees (server clock)
+    with pytest.raises(g.GargantuaError) as e:
+        server.submit(g.RequestSpec(320, 180, 256, 0.5, flags=g.types.REQUEST_BAKE))
+    assert e.value.status == 8
+    server.close()
