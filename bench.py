@@ -614,7 +614,7 @@ def main():
     slices = [stream[i * B:(i + 1) * B] for i in range(nslices)]
     assert all(len(sl) == B for sl in slices), "every slice is full"
     lat_stream = stream[nslices * B:nslices * B + args.latency_requests]
-    shape = {"chunk_rays": 32, "wave_rays": 4 << 20, "max_waves_in_flight": 2, "steps_per_round": 8, "refill_idle": 8,
+    shape = {"chunk_rays": 32, "wave_rays": 4 << 20, "max_waves_in_flight": 6, "steps_per_round": 8, "refill_idle": 8,
              "schedule": 0,
              "chosen_by": "defaults"}
     if not args.no_tune:

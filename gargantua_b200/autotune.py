@@ -25,7 +25,7 @@ from . import types as T
 
 CHUNKS = (32, 64, 128)
 WAVES = (2 << 20, 4 << 20, 8 << 20)
-IN_FLIGHT = (2, 3)
+IN_FLIGHT = (3, 6, 8)
 CADENCES = ((8, 8), (4, 4), (16, 8), (8, 16))  # (steps_per_round, refill_idle)
 SCHEDULES = (T.SCHEDULE_CHUNKS, T.SCHEDULE_LANE_REFILL)
 

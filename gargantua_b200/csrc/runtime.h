@@ -101,6 +101,9 @@ double disk_shape(double r, double floor);
 // Sweep tables (tables.cu).
 int sweep_init(gg_context* ctx);
 int sweep_build(gg_context* ctx, cudaStream_t stream, double camera_radius, gg_sweep* out);
+// The camera and sky tables of `count` camera radii, one launch per 128.
+int sweep_build_batch(gg_context* ctx, cudaStream_t stream, const double* camera_radius, gg_sweep* const* out,
+                      int count);
 void sweep_apply(const gg_context* ctx, const gg_sweep* sweep, MarchUniforms* u);
 
 // Blackbody table on the device (present.cu).

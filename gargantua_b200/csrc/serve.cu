@@ -458,7 +458,8 @@ struct gg_server {
     int injected = GG_OK;  // gg_server_inject_fault: the next device call "fails" with this status
     std::thread worker;
     // total_launches: kernels launched (each wave's two persistent kernels and
-    // its FP64 pass, each Schwarzschild request's two sweep-table builds, one
+    // its FP64 pass, one sweep-table build per admission round (per 128
+    // Schwarzschild requests), two per bake request, one
     // image kernel per request in the plain modes).
     uint64_t total_requests = 0, total_steps = 0, total_launches = 0;
     std::vector<std::pair<double, double>> intervals;  // wave device intervals, seconds after `origin`
@@ -506,7 +507,6 @@ static const gg_volume* request_volume(const gg_server* s, const ServedRequest& 
 static bool serial(const gg_server* s) { return s->cfg.mode != GG_SERVE_BATCHED; }
 
 static int admit(gg_server* s, const std::shared_ptr<ServedRequest>& r) {
-    gg_context* ctx = s->ctx;
     const uint64_t px = r->rays;
     GG_CUDA(cudaMallocFromPoolAsync((void**)&r->d_color, px * 8u, s->pool, s->build), "request target");
     if (r->q.debug_output)
@@ -527,11 +527,29 @@ static int admit(gg_server* s, const std::shared_ptr<ServedRequest>& r) {
                 "camera table");
         GG_CUDA(cudaMallocFromPoolAsync((void**)&r->sweep.sky, SWEEP_TABLE_SIZE * sizeof(float), s->pool, s->build),
                 "sky table");
-        GG_CHECK(sweep_build(ctx, s->build, (double)r->q.distance, &r->sweep));
-        sweep_apply(ctx, &r->sweep, &r->u);
-        s->total_launches += 2;
+        // Its tables are built with those of the other requests admitted
+        // in the same round (build_admitted_tables).
     }
     r->result.admitted = now_seconds();
+    return GG_OK;
+}
+
+// The camera and sky tables of every Schwarzschild request admitted in one
+// round, in one launch on the build stream (per 128 requests), then each
+// request's uniforms take its tables (DeflectionTables.apply).
+static int build_admitted_tables(gg_server* s, const std::vector<std::shared_ptr<ServedRequest>>& round) {
+    std::vector<double> radii;
+    std::vector<gg_sweep*> sweeps;
+    for (auto& r : round)
+        if (r->q.spin == 0.0f) {
+            radii.push_back((double)r->q.distance);
+            sweeps.push_back(&r->sweep);
+        }
+    if (radii.empty()) return GG_OK;
+    GG_CHECK(sweep_build_batch(s->ctx, s->build, radii.data(), sweeps.data(), (int)radii.size()));
+    s->total_launches += (radii.size() + 127u) / 128u;
+    for (auto& r : round)
+        if (r->q.spin == 0.0f) sweep_apply(s->ctx, &r->sweep, &r->u);
     return GG_OK;
 }
 
@@ -774,7 +792,7 @@ static void worker_loop(gg_server* s) {
     for (bool running = true; running;) {
         int status = GG_OK;
         // Admission in arrival order while the footprint fits.
-        bool admitted_any = false;
+        std::vector<std::shared_ptr<ServedRequest>> round;
         while (!s->pending.empty() && s->memory_used + s->pending.front()->footprint <= s->cfg.memory_bytes &&
                (!serial(s) || s->admitted.empty())) {
             auto r = s->pending.front();
@@ -783,9 +801,10 @@ static void worker_loop(gg_server* s) {
             status = admit(s, r);
             if (status != GG_OK) break;
             s->admitted.push_back(r);
-            admitted_any = true;
+            round.push_back(r);
         }
-        if (status == GG_OK && admitted_any) status = cuda_status(cudaEventRecord(s->built, s->build), "admission");
+        if (status == GG_OK && !round.empty()) status = build_admitted_tables(s, round);
+        if (status == GG_OK && !round.empty()) status = cuda_status(cudaEventRecord(s->built, s->build), "admission");
         // Launch work.
         if (status == GG_OK) {
             if (serial(s)) {
@@ -906,8 +925,8 @@ GG_API int gg_server_create(gg_context* ctx, const gg_volume* vol, const gg_serv
                         (unsigned long long)s->cfg.memory_bytes, (unsigned long long)(ctx->budget - ctx->used));
     if (s->cfg.wave_rays == 0) s->cfg.wave_rays = 4u << 20;
     if (s->cfg.chunk_rays == 0) s->cfg.chunk_rays = 32;
-    if (s->cfg.max_waves_in_flight == 0) s->cfg.max_waves_in_flight = 2;
-    if (s->cfg.max_waves_in_flight > 4) s->cfg.max_waves_in_flight = 4;
+    if (s->cfg.max_waves_in_flight == 0) s->cfg.max_waves_in_flight = 6;
+    if (s->cfg.max_waves_in_flight > 8) s->cfg.max_waves_in_flight = 8;
     if (s->cfg.chunk_rays < 32 || s->cfg.chunk_rays > 65536)
         return gg::fail(GG_ERR_INVALID_ARGUMENT, "chunk_rays %u is outside 32..65536.", s->cfg.chunk_rays);
     s->max_chunks = s->cfg.wave_rays / s->cfg.chunk_rays + 1024;

@@ -470,7 +470,7 @@ typedef struct {
     uint64_t memory_bytes;     /* device memory for admitted requests' targets; 0: a quarter of the budget left */
     uint32_t wave_rays;        /* rays packed into one persistent launch; 0: 4 Mi */
     uint32_t chunk_rays;       /* rays per work-stealing chunk; 0: 32, one per lane of a warp */
-    uint32_t max_waves_in_flight; /* 0: 2 */
+    uint32_t max_waves_in_flight; /* 0: 6; at most 8 */
     uint32_t fp64_policy;      /* gg_fp64_policy */
     uint32_t steps_per_round;  /* lane refill: RK4 steps a warp takes between refills of idle lanes; 0: 8 */
     uint32_t refill_idle;      /* lane refill: idle lanes of a warp that trigger a refill; 0: 8 */
@@ -503,7 +503,8 @@ GG_API int gg_server_wait(gg_server* s, uint64_t ticket, double timeout_s, gg_re
 
 /* Totals since creation or the last reset: requests completed, ray steps,
  * kernel launches (each wave's two persistent kernels and its FP64 pass,
- * each Schwarzschild request's two sweep-table builds, or one image kernel
+ * one sweep-table build per admission round of Schwarzschild requests, two
+ * kernels per bake request, or one image kernel
  * per request in the plain modes), device-busy
  * seconds (union of the launches' CUDA-event intervals) and device span
  * seconds (first launch start to last launch end, on the device clock).
