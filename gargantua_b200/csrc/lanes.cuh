@@ -556,6 +556,7 @@ template <typename R> struct KLane {
     KState<R> s, c;
     KConst<R> k;
     R st, ct;  // sin and cos of s.th
+    R sp, cp;  // sin and cos of s.ph (FP32: carried between steps, see k_step)
     R carter0, scale, capture;
     R gauge;  // max of k_gauge over the states after steps 1 .. steps-1
     float3 color;
@@ -600,6 +601,12 @@ template <typename R> __device__ __forceinline__ V3<R> k_position(const KLane<R>
     return v3<R>(radial * l.st * cp, radial * l.st * sp, l.s.r * l.ct);
 }
 
+// The position from the lane's carried sin and cos of the azimuth.
+template <typename R> __device__ __forceinline__ V3<R> k_position_carried(const KLane<R>& l) {
+    R radial = asqrt(fmaT(l.s.r, l.s.r, l.k.a2));
+    return v3<R>(radial * l.st * l.cp, radial * l.st * l.sp, l.s.r * l.ct);
+}
+
 // Direction of travel against the spherical frame (Kerr.h:158-173) from the
 // lane's state, with the sines and cosines the step already has and
 // reciprocals in place of the divides.
@@ -639,7 +646,7 @@ __device__ __forceinline__ void k_init(KLane<R>& l, V3<R> origin, V3<R> directio
     l.transmittance = 1.0f;
     l.travelled = l.weighted_depth = l.depth_weight = 0.0f;
     fast_sincos(l.s.th, &l.st, &l.ct);
-    l.previous = k_position(l);
+    l.previous = k_position(l, &l.sp, &l.cp);
     l.steps = l.samples = 0;
     l.outcome = RayExhausted;
     l.min_r = (float)l.s.r;
@@ -703,8 +710,19 @@ __device__ __forceinline__ bool k_step(KLane<R>& l, const MarchUniforms& u, cuda
     l.steps += 1u;
     fast_sincos(l.s.th, &l.st, &l.ct);
     if constexpr (Project) k_project(l);
-    R sp, cp;
-    V3<R> position = k_position(l, &sp, &cp);
+    // The azimuth enters only the Cartesian position (the metric is
+    // axisymmetric), so in FP32 its sine and cosine are carried: rotated
+    // through the step's own increment (|delta| <= 0.02: the short series of
+    // sincos_shift, remainders below 3e-11), reduced afresh every 16 steps
+    // and after any larger increment, so rounding does not build up.
+    if constexpr (sizeof(R) == 4) {
+        if ((l.steps & 15u) == 0u || !(gabs(inc.ph) <= R(0.02)) || !sincos_shift(l.sp, l.cp, inc.ph, &l.sp, &l.cp))
+            fast_sincos(l.s.ph, &l.sp, &l.cp);
+    } else {
+        fast_sincos(l.s.ph, &l.sp, &l.cp);
+    }
+    const R sp = l.sp, cp = l.cp;
+    V3<R> position = k_position_carried(l);
     V3<R> d = position - l.previous;
     float path = (float)asqrt(dot(d, d));
     l.travelled += path;
