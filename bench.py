@@ -58,7 +58,7 @@ FLOPS_KERR_STEP = 515           # RK4 436 + step policy, position, path, Carter 
 FLOPS_SAMPLE = 111              # in-slab gather 67 + static-observer direction 44
 # DRAM bytes of one serve_kerr_chunks_kernel launch (ncu, 1920x1080 4096-step Kerr still): the
 # march reads only its descriptors and tables from HBM; pixels stay in L2 until the copy-out.
-SERVE_KERR_TRAFFIC_BYTES = 5835776
+SERVE_KERR_TRAFFIC_BYTES = 5836288
 
 
 def stream_length(warmup: int, steps: int, per_step: int, latency_requests: int) -> int:
