@@ -555,9 +555,10 @@ static int build_admitted_tables(gg_server* s, const std::vector<std::shared_ptr
 
 static void release(gg_server* s, ServedRequest& r) {
     if (r.bake) {
-        cudaFreeAsync(r.d_samples, s->copy);
-        cudaFreeAsync(r.d_headers, s->copy);
-        cudaFreeAsync(r.d_overflow, s->copy);
+        // An admission that failed part-way leaves some of these null.
+        if (r.d_samples) cudaFreeAsync(r.d_samples, s->copy);
+        if (r.d_headers) cudaFreeAsync(r.d_headers, s->copy);
+        if (r.d_overflow) cudaFreeAsync(r.d_overflow, s->copy);
         r.d_samples = nullptr;
         r.d_headers = nullptr;
         r.d_overflow = nullptr;
