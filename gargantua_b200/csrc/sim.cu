@@ -32,11 +32,13 @@ struct SimArgs {
 };
 
 // Unnormalized thin-disk profile (Common.h:49-53) with the powers as square
-// roots: x^(3/4) = sqrt(x) sqrt(sqrt(x)), t^(1/4) = sqrt(sqrt(t)).
+// roots: x^(3/4) t^(1/4) = sqrt(x) sqrt(sqrt(x t)), sqrt(x) shared with the
+// zero-torque factor.
 __device__ __forceinline__ float disk_shape_f(float r) {
     float x = R_ISCO / r;
-    float torque = fmaxf(1.0f - sqrtf(x), ZERO_TORQUE_FLOOR);
-    return gg_pow34f(x) * gg_pow14f(torque);
+    float h = sqrtf(x);
+    float torque = fmaxf(1.0f - h, ZERO_TORQUE_FLOOR);
+    return gg_disk_powers(x, h, torque);
 }
 
 __device__ __forceinline__ float square3(float x, float y, float z) { return x * x + y * y + z * z; }

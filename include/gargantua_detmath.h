@@ -149,4 +149,10 @@ GG_HD float gg_pow34f(float x) {
 /* x^(1/4) for x >= 0. */
 GG_HD float gg_pow14f(float x) { return sqrtf(sqrtf(x)); }
 
+/* The thin-disk profile's powers x^(3/4) t^(1/4) (Common.h:49-53) for x, t
+ * >= 0, given h = sqrt(x) (which the profile's zero-torque factor has
+ * computed already): h (x t)^(1/4), three square roots in all where the
+ * separate powers take four. */
+GG_HD float gg_disk_powers(float x, float h, float t) { return h * sqrtf(sqrtf(x * t)); }
+
 #endif

@@ -47,8 +47,9 @@ static float circular_speedf(float r, uint32_t potential) { return sqrtf(r * gra
 
 static float disk_shapef(float r) {
     float x = R_ISCO / r;
-    float torque = fmaxf(1.0f - sqrtf(x), ZERO_TORQUE_FLOOR);
-    return gg_pow34f(x) * gg_pow14f(torque);
+    float h = sqrtf(x);
+    float torque = fmaxf(1.0f - h, ZERO_TORQUE_FLOOR);
+    return gg_disk_powers(x, h, torque);
 }
 
 static float length3f(float x, float y, float z) { return sqrtf(x * x + y * y + z * z); }
