@@ -209,6 +209,7 @@ def still(o: Options) -> None:
     print(f"served {o.width} by {o.height}: {res.ray_steps} ray steps, {res.fp64_rays} rays re-integrated in FP64, "
           f"device {span * 1e3:.2f} ms ({res.ray_steps / span / 1e9:.2f} G ray-steps/s), wall {wall * 1e3:.1f} ms",
           flush=True)
+    print_counters(res.counters)
     server.close()
     targets = H.Targets(ctx, o.width, o.height)
     targets.write(color=pixels)
@@ -219,6 +220,21 @@ def still(o: Options) -> None:
     H.write_png(o.still_path, rgba)
     print(f"still {os.path.abspath(o.still_path)}", flush=True)
     ctx.close()
+
+
+def counters_line(c) -> str | None:
+    """The HUD's validation line (Renderer.swift:133-137) for a frame's
+    MarchCounters; None when no ray was marched."""
+    if c.rays == 0:
+        return None
+    return (f"drift over budget {100.0 * c.overDriftBudget / c.rays:.2f} percent, {c.exhausted} exhausted, "
+            f"{c.captured} captured")
+
+
+def print_counters(c) -> None:
+    line = counters_line(c)
+    if line:
+        print(line, flush=True)
 
 
 def _sequence(ctx, ps, vol, cam, o: Options) -> None:
@@ -234,7 +250,7 @@ def _sequence(ctx, ps, vol, cam, o: Options) -> None:
         u = H.uniforms(cam, 960, 540, H.Settings.interactive(), H.DRIFT_BUDGET_INTERACTIVE, True, o.seed, spin=o.spin)
         if o.spin == 0.0:
             ctx.enable_tables(u, float(cam.distance))
-        H.march(ctx, vol, u, targets)
+        print_counters(H.march(ctx, vol, u, targets))
         H.write_png(os.path.join(folder, f"seq-{frame:03d}.png"), targets.tonemap())
     targets.close()
     print(f"sequence of {o.sequence} frames beside the still", flush=True)

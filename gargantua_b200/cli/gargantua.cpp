@@ -291,6 +291,14 @@ std::string folder_of(const std::string& path) {
     return slash == std::string::npos ? std::string(".") : path.substr(0, slash);
 }
 
+// The HUD's validation line (Renderer.swift:133-137) for one frame's
+// counters, printed per served still and sequence frame.
+void print_counters(const MarchCounters& c) {
+    if (c.rays == 0) return;
+    std::printf("drift over budget %.2f percent, %u exhausted, %u captured\n",
+                100.0 * (double)c.overDriftBudget / (double)c.rays, c.exhausted, c.captured);
+}
+
 // Still.render (Still.swift:8-98), the march served as one request.
 void still(const Options& o) {
     Scene s;
@@ -329,6 +337,7 @@ void still(const Options& o) {
                 "wall %.1f ms\n",
                 o.width, o.height, (unsigned long long)res.ray_steps, (unsigned long long)res.fp64_rays, span * 1e3,
                 (double)res.ray_steps / span / 1e9, wall * 1e3);
+    print_counters(res.counters);
     gg_targets* t = nullptr;
     check(gg_targets_create(s.ctx, o.width, o.height, &t));
     status = gg_targets_write(t, pixels.data(), nullptr);
@@ -351,7 +360,9 @@ void still(const Options& o) {
                 s.splat(o.seed, false);
                 MarchUniforms u = march_uniforms(o, 960, 540, false, DRIFT_BUDGET_INTERACTIVE);
                 if (o.spin == 0.0) check(gg_tables_update(s.ctx, (float)o.distance, &u));
-                check(gg_march(s.ctx, s.vol, &u, ft, GG_PRECISION_PLAIN, nullptr));
+                MarchCounters counters;
+                check(gg_march(s.ctx, s.vol, &u, ft, GG_PRECISION_PLAIN, &counters));
+                print_counters(counters);
                 char name[32];
                 std::snprintf(name, sizeof name, "/seq-%03u.png", frame);
                 write_tonemapped(ft, 960, 540, DRIFT_BUDGET_INTERACTIVE, folder_of(o.still_path) + name);

@@ -98,3 +98,13 @@ def test_host_writers_refuse_arrays_of_the_wrong_size():
         expect_size(np.zeros(31), 32, "records")
     with pytest.raises(ValueError):
         write_png("unused.png", np.zeros((4, 4), np.uint8))
+
+
+def test_counters_line_is_the_huds():
+    """Renderer.swift:133-137: percent over the drift budget, exhausted and
+    captured rays; nothing for a frame with no rays."""
+    from gargantua_b200 import types as T
+
+    c = T.MarchCounters(rays=2000, overDriftBudget=31, exhausted=4, captured=250)
+    assert cli.counters_line(c) == "drift over budget 1.55 percent, 4 exhausted, 250 captured"
+    assert cli.counters_line(T.MarchCounters()) is None

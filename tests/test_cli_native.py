@@ -63,6 +63,7 @@ def test_still_writes_a_png(exe, tmp_path):
     assert data[:8] == b"\x89PNG\r\n\x1a\n" and len(data) > 1000
     assert (tmp_path / "seq-000.png").exists() and (tmp_path / "seq-001.png").exists()
     assert "served 320 by 180" in r.stdout
+    assert r.stdout.count("drift over budget") == 3  # the still and each of the 2 frames (the HUD's line)
 
 
 @pytest.mark.gpu
