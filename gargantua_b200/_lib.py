@@ -23,6 +23,7 @@ STATUS = {
     6: "not ready",
     7: "no device",
     8: "unsupported",
+    9: "cancelled",
 }
 
 
@@ -108,6 +109,7 @@ SIGNATURES = {
     "gg_server_submit": (i, [vp, P(T.Request), P(u64)]),
     "gg_server_inject_fault": (i, [vp, i]),
     "gg_server_poll": (i, [vp, u64, P(i)]),
+    "gg_server_cancel": (i, [vp, u64]),
     "gg_server_wait": (i, [vp, u64, C.c_double, P(T.RequestResult)]),
     "gg_server_totals": (i, [vp, i, P(u64), P(u64), P(u64), P(C.c_double), P(C.c_double)]),
     "gg_measure_fp32_peak": (i, [vp, P(C.c_double)]),

@@ -192,6 +192,7 @@ GG_API const char* gg_status_name(int status) {
         case GG_ERR_NOT_READY: return "not ready";
         case GG_ERR_NO_DEVICE: return "no device";
         case GG_ERR_UNSUPPORTED: return "unsupported";
+        case GG_ERR_CANCELLED: return "cancelled";
         default: return "unknown status";
     }
 }

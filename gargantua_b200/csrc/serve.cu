@@ -1098,6 +1098,24 @@ GG_API int gg_server_inject_fault(gg_server* s, int status) {
     return GG_OK;
 }
 
+GG_API int gg_server_cancel(gg_server* s, uint64_t ticket) {
+    if (!s) return gg::fail(GG_ERR_INVALID_ARGUMENT, "gg_server_cancel needs a server.");
+    std::lock_guard<std::mutex> lock(s->mu);
+    auto it = s->all.find(ticket);
+    if (it == s->all.end()) return gg::fail(GG_ERR_INVALID_ARGUMENT, "Unknown ticket %llu.", (unsigned long long)ticket);
+    auto r = it->second;
+    auto p = std::find(s->pending.begin(), s->pending.end(), r);
+    if (p == s->pending.end())
+        return gg::fail(GG_ERR_NOT_READY, "Request %llu is %s; it completes.", (unsigned long long)ticket,
+                        r->done ? "already done" : "admitted and on the device");
+    s->pending.erase(p);
+    r->result.status = GG_ERR_CANCELLED;
+    r->result.finished = gg::now_seconds();
+    r->done = true;
+    s->cv_done.notify_all();
+    return GG_OK;
+}
+
 GG_API int gg_server_poll(gg_server* s, uint64_t ticket, int* done) {
     if (!s || !done) return gg::fail(GG_ERR_INVALID_ARGUMENT, "gg_server_poll needs a server and an output.");
     std::lock_guard<std::mutex> lock(s->mu);
@@ -1120,6 +1138,8 @@ GG_API int gg_server_wait(gg_server* s, uint64_t ticket, double timeout_s, gg_re
     if (!ok) return gg::fail(GG_ERR_TIMEOUT, "Request %llu is not done after %g s.", (unsigned long long)ticket, timeout_s);
     if (result) *result = r->result;
     s->all.erase(it);
+    if (r->result.status == GG_ERR_CANCELLED)
+        return gg::fail(GG_ERR_CANCELLED, "Request %llu was cancelled before admission.", (unsigned long long)ticket);
     return GG_OK;
 }
 

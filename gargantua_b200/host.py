@@ -686,11 +686,20 @@ class Server:
         return bool(d.value)
 
     def wait(self, ticket: int, timeout_s: float = 600.0):
-        """(pixels, debug-or-None, RequestResult)."""
+        """(pixels, debug-or-None, RequestResult). A cancelled request raises
+        GargantuaError with status GG_ERR_CANCELLED (9)."""
         res = T.RequestResult()
-        check(lib().gg_server_wait(self.handle, ticket, timeout_s, C.byref(res)))
+        status = lib().gg_server_wait(self.handle, ticket, timeout_s, C.byref(res))
+        if status == 9:  # the library forgot the ticket: so do its buffers
+            self._buffers.pop(ticket, None)
+        check(status)
         out, dbg = self._buffers.pop(ticket)
         return out, dbg, res
+
+    def cancel(self, ticket: int) -> None:
+        """gg_server_cancel: withdraw a request still waiting for admission
+        (GargantuaError with GG_ERR_NOT_READY once it is admitted)."""
+        check(lib().gg_server_cancel(self.handle, ticket))
 
     def totals(self, reset: bool = False):
         a, b, c, d, e = C.c_uint64(), C.c_uint64(), C.c_uint64(), C.c_double(), C.c_double()
@@ -733,6 +742,25 @@ class Sequence:
 
     def run(self):
         return [self.frame() for _ in range(self.frames)]
+
+    def snapshot(self) -> dict:
+        """The sequence's state between frames: the particle records (the AoS
+        Particle layout), their FNV-1a checksum (Validate.swift:378-387) and
+        the splat's frame counter. Every later random draw is pcg4d(index,
+        event, seed), so this is all a resume needs."""
+        return {"particles": self.particles.read(), "checksum": self.particles.checksum(),
+                "splat_frame": self.volume.frame}
+
+    def restore(self, snap: dict) -> None:
+        """Resume from snapshot(): the particle records are written back and
+        checked against the snapshot's checksum, and the splat's frame
+        counter is restored, so the following frames are the ones the
+        snapshotted sequence would have rendered, bit for bit."""
+        self.particles.write(snap["particles"])
+        got = self.particles.checksum()
+        if got != snap["checksum"]:
+            raise ValueError(f"particle checksum {got:016x} does not match the snapshot's {snap['checksum']:016x}")
+        self.volume.frame = int(snap["splat_frame"])
 
     def close(self):
         self.volume.close()

@@ -40,7 +40,8 @@ typedef enum {
     GG_ERR_TIMEOUT = 5,
     GG_ERR_NOT_READY = 6,
     GG_ERR_NO_DEVICE = 7,
-    GG_ERR_UNSUPPORTED = 8
+    GG_ERR_UNSUPPORTED = 8,
+    GG_ERR_CANCELLED = 9     /* a served request withdrawn by gg_server_cancel */
 } gg_status;
 
 typedef struct gg_context gg_context;
@@ -496,6 +497,12 @@ GG_API int gg_server_submit(gg_server* s, const gg_request* req, uint64_t* ticke
 GG_API int gg_server_inject_fault(gg_server* s, int status);
 
 GG_API int gg_server_poll(gg_server* s, uint64_t ticket, int* done);
+
+/* Withdraw a request that is still waiting for admission: it never runs,
+ * and gg_server_wait on it returns GG_ERR_CANCELLED (and forgets the
+ * ticket). A request already admitted has its rays on the device and
+ * completes: GG_ERR_NOT_READY, nothing changes. No reference counterpart. */
+GG_API int gg_server_cancel(gg_server* s, uint64_t ticket);
 
 /* Block until the request completes or timeout_s passes (GG_ERR_TIMEOUT);
  * on success fills *result (may be NULL) and forgets the ticket. */

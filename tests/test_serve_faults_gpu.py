@@ -7,7 +7,7 @@ import pytest
 
 pytestmark = pytest.mark.gpu
 
-GG_ERR_OVER_BUDGET, GG_ERR_DEVICE, GG_ERR_TIMEOUT = 3, 4, 5
+GG_ERR_OVER_BUDGET, GG_ERR_DEVICE, GG_ERR_TIMEOUT, GG_ERR_NOT_READY, GG_ERR_CANCELLED = 3, 4, 5, 6, 9
 
 
 @pytest.fixture(scope="module")
@@ -68,6 +68,46 @@ def test_request_larger_than_the_server_is_refused(world):
     with pytest.raises(g.GargantuaError) as e:
         server.submit(g.RequestSpec(3840, 2160, 256))
     assert e.value.status == GG_ERR_OVER_BUDGET
+    _, _, res = server.wait(server.submit(g.RequestSpec(320, 180, 256)))
+    assert res.status == 0
+    server.close()
+
+
+def test_pending_requests_can_be_cancelled(world):
+    """Request cancellation (host side): with memory for one request at a
+    time, the requests queued behind it are withdrawn before admission --
+    their waits report GG_ERR_CANCELLED, they never run -- while the one
+    already admitted cannot be (GG_ERR_NOT_READY) and completes; the server
+    then serves new work."""
+    import gargantua_b200 as g
+
+    ctx, vol = world
+    spec = g.RequestSpec(1920, 1080, 4096, 0.9)
+    one = 1920 * 1080 * 8 + 128 + 8192
+    server = g.Server(ctx, vol, g.types.SERVE_BATCHED, memory_bytes=int(one * 1.5))
+    tickets = [server.submit(spec) for _ in range(4)]
+    cancelled = []
+    for t in tickets[1:]:
+        try:
+            server.cancel(t)
+            cancelled.append(t)
+        except g.GargantuaError as e:
+            assert e.status == GG_ERR_NOT_READY  # admitted before the cancel reached it
+    assert cancelled, "at least the last request was still waiting"
+    with pytest.raises(g.GargantuaError) as e:
+        server.cancel(tickets[0])
+    assert e.value.status == GG_ERR_NOT_READY
+    for t in tickets:
+        if t in cancelled:
+            with pytest.raises(g.GargantuaError) as e:
+                server.wait(t, timeout_s=60.0)
+            assert e.value.status == GG_ERR_CANCELLED
+        else:
+            _, _, res = server.wait(t, timeout_s=120.0)
+            assert res.status == 0 and res.counters.rays == 1920 * 1080
+    assert server.totals()["requests"] == len(tickets) - len(cancelled)
+    with pytest.raises(g.GargantuaError):
+        server.cancel(tickets[0])  # forgotten after its wait
     _, _, res = server.wait(server.submit(g.RequestSpec(320, 180, 256)))
     assert res.status == 0
     server.close()

@@ -258,6 +258,35 @@ def test_schedules_give_the_same_pixels(world):
         assert np.abs(la - lb).sum() / max(lb.sum(), 1e-30) < 1e-5
 
 
+def test_a_sequence_resumes_from_its_snapshot(world):
+    """Checkpoint and resume of a served sequence: a second sequence
+    restored from the first one's snapshot after two frames renders the
+    first one's frames three and four bit for bit (the particle records are
+    checked against their FNV-1a checksum on restore; every later random
+    draw is keyed on index, event and seed)."""
+    import gargantua_b200 as g
+
+    ctx = world["ctx"]
+    server = g.Server(ctx, world["vol"], g.types.SERVE_BATCHED)
+    first = g.Sequence(server, ctx, 40_000, 48, frames=4, width=320, height=180, seed=6, settle_dispatches=20)
+    frames = [first.frame()[0] for _ in range(2)]
+    snap = first.snapshot()
+    frames += [first.frame()[0] for _ in range(2)]
+    second = g.Sequence(server, ctx, 40_000, 48, frames=2, width=320, height=180, seed=6, settle_dispatches=1)
+    second.restore(snap)
+    for k in (2, 3):
+        pixels, res = second.frame()
+        assert res.status == 0
+        assert np.array_equal(pixels.view(np.uint16), frames[k].view(np.uint16)), k
+    assert first.particles.checksum() == second.particles.checksum()
+    bad = dict(snap, checksum=snap["checksum"] ^ 1)
+    with pytest.raises(ValueError):
+        second.restore(bad)
+    first.close()
+    second.close()
+    server.close()
+
+
 def test_bake_requests_are_served_beside_marches(world):
     """GG_REQUEST_BAKE (the bake strategy as a served request): the walk of
     its bake renders the march's image of the same camera (image light
