@@ -542,3 +542,68 @@ def test_edge_measurement_recovers_analytic_profile():
     radii = table[k] + (pos - k) * (table[k + 1] - table[k])
     edge = L.o_disk_inner_edge(np.ascontiguousarray(radii), n, 0.25, 6.5, 9.0)
     assert abs(edge - 6.0) < 0.1
+
+
+def test_bake_oracle_follows_the_integrator():
+    """The FP64 bake (o_bake_batch, bake.metal:46-91 in the oracle's
+    integrator) steps exactly as o_integrate does: a ray's final direction
+    is the integrator's, every stored point lies in the slab at least the
+    spacing of path after the previous one, and the stored paths add up to
+    at most the path walked (the rest is after the last stored point)."""
+    rng = np.random.default_rng(4)
+    cam = np.array([40.0, 20.0, 16.0])
+    fwd = -cam / np.linalg.norm(cam)
+    dirs = fwd + rng.normal(scale=0.12, size=(48, 3))
+    dirs /= np.linalg.norm(dirs, axis=1, keepdims=True)
+    probes = np.concatenate([np.broadcast_to(cam, dirs.shape), dirs], axis=1)
+    spacing = 0.234375
+    samples, counts, over, falls, dd = O.bake_batch(probes, O.still(), spacing, threads=1)
+    ref = O.integrate_batch(probes, O.still(), 1)
+    assert counts.max() > 0 and (counts <= 96).all()
+    for i in range(len(probes)):
+        n = counts[i]
+        if ref[i, 7] != O.CAPTURED:
+            assert np.allclose(dd[i, :3], ref[i, 3:6], rtol=0, atol=1e-12), i
+        pts = samples[i, :n]
+        assert (np.abs(pts[:, 2]) < 6.0).all() and (np.abs(pts[:, :2]) < 30.0).all()
+        assert (pts[:, 3] >= spacing).all()
+        assert 0.0 <= dd[i, 3] <= 1.0
+    assert set(np.unique(falls)) <= {0, 1}
+    assert (falls[ref[:, 7] == O.CAPTURED] == 1).all()
+
+
+def test_present_replica_matches_the_fp64_tone_curve():
+    """The FP32 tone-curve replica (o32_present + o32_srgb8, the kernel's
+    arithmetic) against PBR Neutral in FP64 (o_pbr_neutral, present.metal:
+    22-35) encoded to sRGB in FP64: within one code value everywhere."""
+    rng = np.random.default_rng(8)
+    rgba = rng.uniform(0.0, 4.0, (4000, 4)).astype(np.float16)
+    rgba[::5] = rng.uniform(0.0, 0.09, (len(rgba[::5]), 4)).astype(np.float16)
+    got = O.present32(rgba, 1.3)
+    want = np.zeros((len(rgba), 3))
+    for k, row in enumerate(rgba.astype(np.float64)):
+        out = np.zeros(3)
+        O.lib().o_pbr_neutral(np.ascontiguousarray(np.maximum(row[:3] * float(np.float32(1.3)), 0.0)), out)
+        v = np.clip(out, 0.0, 1.0)
+        want[k] = np.round(np.where(v <= 0.0031308, 12.92 * v, 1.055 * v ** (1 / 2.4) - 0.055) * 255.0)
+    assert np.abs(got[:, :3].astype(np.float64) - want).max() <= 1.0
+    assert (got[:, 3] == 255).all()
+
+
+def test_threaded_replicas_equal_the_serial_ones():
+    """The CPU baseline's all-core deposit (atomic adds of the same integer
+    words) and resolve (independent voxels) give the serial replica's
+    outputs bit for bit."""
+    rng = np.random.default_rng(1)
+    n = 100_000
+    p = np.zeros((n, 8), np.float32)
+    p[:, :3] = rng.uniform(-31, 31, (n, 3))
+    p[:, 3:6] = rng.normal(0, 1, (n, 3))
+    p[:, 6] = rng.uniform(1000, 12000, n)
+    for exact in (True, False):
+        a = O.deposit32(p, 40, 3, exact, 1)
+        b = O.deposit32(p, 40, 3, exact, 1, threads=0)
+        assert all(np.array_equal(x, y) for x, y in zip(a, b))
+    bb = np.random.default_rng(2).uniform(0, 1, (256, 3)).astype(np.float32)
+    r1, r2 = O.resolve32(*a, 40, bb), O.resolve32(*a, 40, bb, threads=0)
+    assert all(np.array_equal(x.view(np.uint32), y.view(np.uint32)) for x, y in zip(r1, r2))
