@@ -271,6 +271,7 @@ GG_API void gg_bake_destroy(gg_bake* b) {
 }
 
 GG_API int gg_bake_rows(gg_bake* b, const MarchUniforms* u, uint32_t row_begin, uint32_t row_end) {
+    gg::Range range("gg_bake_rows");
     if (!b) return gg::fail(GG_ERR_INVALID_ARGUMENT, "gg_bake_rows needs a bake.");
     gg_context* ctx = b->ctx;
     std::lock_guard<std::recursive_mutex> lock(ctx->mu);
@@ -311,6 +312,7 @@ GG_API int gg_bake_overflow(gg_bake* b, uint32_t* count, int reset) {
 }
 
 GG_API int gg_walk(gg_bake* b, const gg_volume* vol, const MarchUniforms* u, gg_targets* targets) {
+    gg::Range range("gg_walk");
     if (!b || !u || !targets) return gg::fail(GG_ERR_INVALID_ARGUMENT, "gg_walk needs a bake, uniforms and targets.");
     gg_context* ctx = b->ctx;
     std::lock_guard<std::recursive_mutex> lock(ctx->mu);

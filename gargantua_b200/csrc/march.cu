@@ -357,6 +357,7 @@ GG_API int gg_targets_write(gg_targets* t, const uint16_t* color, const uint16_t
 
 GG_API int gg_march(gg_context* ctx, const gg_volume* vol, const MarchUniforms* u, gg_targets* targets, int precision,
                     MarchCounters* counters) {
+    gg::Range range("gg_march");
     if (!ctx || !targets) return gg::fail(GG_ERR_INVALID_ARGUMENT, "gg_march needs a context and targets.");
     if (!gg::known_precision(precision))
         return gg::fail(GG_ERR_INVALID_ARGUMENT, "Unknown precision policy %d.", precision);
@@ -489,6 +490,7 @@ GG_API int gg_capture_boundary(gg_context* ctx, const MarchUniforms* u, const do
 
 GG_API int gg_probe(gg_context* ctx, const MarchUniforms* u, const RayProbe* probes, RayProbeResult* results,
                     uint32_t count, int precision) {
+    gg::Range range("gg_probe");
     if (!ctx || (!probes && count) || (!results && count))
         return gg::fail(GG_ERR_INVALID_ARGUMENT, "gg_probe needs a context and probe arrays.");
     if (!gg::known_precision(precision))

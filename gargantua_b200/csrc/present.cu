@@ -113,6 +113,7 @@ static void chunk(std::vector<uint8_t>& png, const char* type, const uint8_t* da
 extern "C" {
 
 GG_API int gg_tonemap(gg_targets* t, const PresentUniforms* u, uint8_t* rgba8) {
+    gg::Range range("gg_tonemap");
     if (!t || !u || !rgba8) return gg::fail(GG_ERR_INVALID_ARGUMENT, "gg_tonemap needs targets, uniforms and an output.");
     gg_context* ctx = t->ctx;
     std::lock_guard<std::recursive_mutex> lock(ctx->mu);

@@ -5,6 +5,7 @@
 
 #include <cuda_runtime.h>
 #include <cuda_fp16.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <algorithm>
 #include <cstdarg>
@@ -16,6 +17,16 @@
 #include "../../include/gargantua_constants.h"
 
 namespace gg {
+
+// A named NVTX range for the scope (the pass entry points and the server's
+// scheduling steps), so a profiler's timeline shows which call launched
+// what. NVTX is header-only and costs a branch when no tool is attached.
+struct Range {
+    explicit Range(const char* name) { nvtxRangePushA(name); }
+    ~Range() { nvtxRangePop(); }
+    Range(const Range&) = delete;
+    Range& operator=(const Range&) = delete;
+};
 
 // Record `status` with a sentence for gg_last_error() and return it.
 int fail(int status, const char* fmt, ...) __attribute__((format(printf, 2, 3)));

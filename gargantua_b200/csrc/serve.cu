@@ -507,6 +507,7 @@ static const gg_volume* request_volume(const gg_server* s, const ServedRequest& 
 static bool serial(const gg_server* s) { return s->cfg.mode != GG_SERVE_BATCHED; }
 
 static int admit(gg_server* s, const std::shared_ptr<ServedRequest>& r) {
+    gg::Range range("serve: admit");
     const uint64_t px = r->rays;
     GG_CUDA(cudaMallocFromPoolAsync((void**)&r->d_color, px * 8u, s->pool, s->build), "request target");
     if (r->q.debug_output)
@@ -673,6 +674,7 @@ static bool form_wave(gg_server* s, WaveSlot& w) {
 }
 
 static int launch_wave(gg_server* s, WaveSlot& w) {
+    gg::Range range("serve: launch wave");
     WaveHeader* hdr = reinterpret_cast<WaveHeader*>(w.host);
     GG_CUDA(cudaStreamWaitEvent(w.stream, s->built, 0), "wave ordering");
     GG_CUDA(cudaMemcpyAsync(w.device, w.host, sizeof(WaveHeader) + hdr->request_count * sizeof(ServeRequest),
@@ -700,6 +702,7 @@ static int launch_wave(gg_server* s, WaveSlot& w) {
 }
 
 static int finish_wave(gg_server* s, WaveSlot& w) {
+    gg::Range range("serve: finish wave");
     // The wave's device interval runs from its start to the end of its FP64
     // pass, which may overlap the next wave.
     float t0 = 0.0f, t1 = 0.0f, t2 = 0.0f;
@@ -722,6 +725,7 @@ static int finish_wave(gg_server* s, WaveSlot& w) {
 // state: the launch's device interval is returned in *interval and the
 // caller records it (and the launch count) once it holds the mutex again.
 static int run_plain(gg_server* s, ServedRequest& r, std::pair<double, double>* interval) {
+    gg::Range range("serve: per-request launch");
     gg_context* ctx = s->ctx;
     if (r.bake) {
         GG_CUDA(cudaEventRecord(s->slots[0].start, s->plain), "plain event");

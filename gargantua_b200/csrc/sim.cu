@@ -307,6 +307,7 @@ GG_API int gg_particles_seed(gg_particles* ps) {
 }
 
 GG_API int gg_particles_step(gg_particles* ps, uint32_t dispatches) {
+    gg::Range range("gg_particles_step");
     GG_CHECK(check_particles(ps, "gg_particles_step"));
     gg_context* ctx = ps->ctx;
     std::lock_guard<std::recursive_mutex> lock(ctx->mu);

@@ -137,9 +137,9 @@ __global__ void __launch_bounds__(256) bin_kernel(SplatArgs a) {
 //            its range of every brick with one atomic, then particle indices
 //            written into brick order;
 //   deposit  one block per work item: the tile's records (six words and a
-//            pad, see kTileStride) zeroed in shared memory, the chunk's particles deposited there with
-//            shared atomics, the non-zero words added to the sums with one
-//            global atomic each.
+//            pad, see kTileStride) zeroed in shared memory, the chunk's
+//            particles deposited there with shared atomics, the non-zero
+//            words added to the sums with one global atomic each.
 // Integer sums do not depend on the order of the adds, so the grid equals
 // the direct kernel's bit for bit.
 
@@ -770,6 +770,7 @@ GG_API int gg_splat_resolve(gg_volume* vol, const SplatUniforms* u, const gg_par
 }
 
 GG_API int gg_splat(gg_particles* ps, gg_volume* vol, const SplatUniforms* u) {
+    gg::Range range("gg_splat");
     GG_CHECK(gg_splat_bin(ps, vol, u));
     return gg_splat_resolve(vol, u, ps);
 }
