@@ -6,8 +6,8 @@ chosen by timing candidates on the caller's own data.
   the volume, per deposit mode.
 * March: the image kernels' thread block, timed on a frame of the caller's
   shape (tune_march_block).
-* Server: each candidate (schedule, chunk_rays, wave_rays,
-  max_waves_in_flight, refill cadence) serves
+* Server: each candidate (chunk_rays, wave_rays, max_waves_in_flight; the
+  schedule and refill cadence when asked for) serves
   the same sample of requests closed-loop on a fresh server; the candidate
   with the smallest device span (first launch to last, CUDA events) wins.
   The sample should look like the traffic to come: sizes, step budgets and
@@ -27,7 +27,11 @@ CHUNKS = (32, 64, 128)
 WAVES = (2 << 20, 4 << 20, 8 << 20)
 IN_FLIGHT = (3, 6, 8)
 CADENCES = ((8, 8), (4, 4), (16, 8), (8, 16))  # (steps_per_round, refill_idle)
-SCHEDULES = (T.SCHEDULE_CHUNKS, T.SCHEDULE_LANE_REFILL)
+# The chunk schedule only, by default: on a 16-request sample the lane-refill
+# schedule once timed fastest by a hair and then served the full stream at
+# 60 G ray-steps/s against the chunk schedule's 80 (B200, 7 blocks per SM).
+# A caller may still tune it in by passing `schedules`.
+SCHEDULES = (T.SCHEDULE_CHUNKS,)
 
 
 @dataclass

@@ -288,12 +288,15 @@ __device__ void serve_chunks(const WaveArgs& a, uint32_t lane) {
 }
 
 // One persistent kernel per metric and schedule; a wave runs the two
-// metrics side by side. All four are held to 5 blocks per SM (at most 102
-// registers; the step needs 96 without spilling): 20 warps per SM instead of
-// 16 served the stream 1.7 % faster than the 119 registers the compiler
-// picks unbounded, and compiling every schedule under the same bound keeps
-// their arithmetic, and so their pixels, identical.
-constexpr int kServeBlocksPerSM = 5;
+// metrics side by side. All four are held to 7 blocks per SM (at most 72
+// registers, with a few dozen bytes of spills): the step is bound by
+// instruction issue, and more warps per SM keep the issue slots fuller.
+// Measured on the mixed stream (64 requests, A/B on one box): 4 blocks per
+// SM 76.9 G ray-steps/s, 5 78.7, 6 79.6, 7 80.4, 8 78.1 (its spills grow to
+// 80 bytes); the compiler unbounded picks 119 registers, 4 blocks. Compiling
+// every schedule under the same bound keeps their arithmetic, and so their
+// pixels, identical.
+constexpr int kServeBlocksPerSM = 7;
 
 __global__ void __launch_bounds__(kServeThreads, kServeBlocksPerSM) serve_schwarzschild_kernel(WaveArgs a) {
     serve_queue<0>(a, threadIdx.x & 31u);
