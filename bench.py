@@ -742,7 +742,11 @@ def main():
     if rank == 0 and world == 1:
         threads = os.cpu_count() or 1
         cv, crays, csteps, csecs, desc = cpu_sample(timed, args.cpu_seconds, threads)
-        cpu = {"value": cv, "unit": "ray-steps/s", "cores": threads, "kind": "port", "sample": desc}
+        # The reference's oracle renders serially (Sources/Oracle/LensedRender.swift:3-5):
+        # the same integrators on one thread, a shorter bounded sample.
+        sv, srays, ssteps, ssecs, sdesc = cpu_sample(timed, max(1.0, args.cpu_seconds / 4), 1)
+        cpu = {"value": cv, "unit": "ray-steps/s", "cores": threads, "kind": "port", "sample": desc,
+               "single_thread": sv, "single_thread_sample": sdesc}
 
     achieved = flops_total / busy / 1e12
     summary = {
