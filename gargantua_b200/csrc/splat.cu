@@ -11,6 +11,8 @@
 // order the atomics arrive in, as long as each corner's fixed-point values
 // are: this translation unit is built with --fmad=false and evaluates every
 // float expression in the order the CPU replica (oracle/replica.c) does.
+#include <algorithm>
+#include <mutex>
 #include <vector>
 
 #include "../../include/gargantua_detmath.h"
@@ -131,15 +133,16 @@ __global__ void __launch_bounds__(256) bin_kernel(SplatArgs a) {
 // fall in that brick's (B+1)^3 tile. Four launches:
 //   count    each particle's brick (its key, stored) and a per-block shared
 //            histogram of keys, summed into global counts;
-//   scan     one block: brick offsets and work items (ceil(count / chunk)
-//            particles-chunks per brick);
+//   scan     one block: brick offsets and the work items, ceil(count /
+//            chunk) chunks of each brick's sorted range, listed in a table;
 //   scatter  the histogram again from the stored keys, each block reserving
 //            its range of every brick with one atomic, then particle indices
 //            written into brick order;
-//   deposit  one block per work item: the tile's records (six words and a
-//            pad, see kTileStride) zeroed in shared memory, the chunk's
-//            particles deposited there with shared atomics, the non-zero
-//            words added to the sums with one global atomic each.
+//   deposit  persistent blocks taking work items from a counter: the tile's
+//            records (six words and a pad, see kTileStride) in shared
+//            memory, the chunk's particles deposited there with shared
+//            atomics, the non-zero words added to the sums with one global
+//            atomic each and zeroed for the next item.
 // Integer sums do not depend on the order of the adds, so the grid equals
 // the direct kernel's bit for bit.
 
@@ -155,6 +158,7 @@ struct BrickArgs {
     SplatUniforms u;
     uint32_t first_index;
     uint32_t edge;       // B
+    uint32_t edge_shift; // log2(B)
     uint32_t per_axis;   // ceil(n / B)
     uint32_t bricks;     // per_axis^3
     uint32_t chunk;      // particles per deposit work item
@@ -165,10 +169,14 @@ struct BrickArgs {
     uint32_t* items;     // [bricks + 1], exclusive scan of ceil(count / chunk)
     uint32_t* sorted;    // [particleCount], particle slots in brick order
     uint32_t* keys;      // [particleCount], each particle's brick (kOutside: none), from the count pass
+    uint4* work;         // [max_items], per work item: brick, first and end sorted slot (from the scan)
+    uint32_t max_items;  // ceil(particleCount / chunk) + bricks, a bound on the work items
+    uint32_t* next;      // the deposit blocks' work counter (zeroed by the scan)
 };
 
 __device__ __forceinline__ uint32_t brick_of(const Footprint& f, const BrickArgs& a) {
-    return ((uint32_t)f.lz / a.edge * a.per_axis + (uint32_t)f.ly / a.edge) * a.per_axis + (uint32_t)f.lx / a.edge;
+    return (((uint32_t)f.lz >> a.edge_shift) * a.per_axis + ((uint32_t)f.ly >> a.edge_shift)) * a.per_axis +
+           ((uint32_t)f.lx >> a.edge_shift);
 }
 
 // Inclusive sum over the warp of a value per lane (shuffle scan).
@@ -243,28 +251,49 @@ __global__ void __launch_bounds__(kScanThreads) brick_scan_kernel(BrickArgs a) {
             a.offsets[b + j] = op;
             a.cursor[b + j] = op;
             a.items[b + j] = oi;
+            // The brick's work items: consecutive chunks of its sorted range.
+            for (uint32_t s = 0; s < c[j];) {
+                const uint32_t len = min(c[j] - s, a.chunk);
+                if (oi < a.max_items) a.work[oi] = make_uint4(b + j, op + s, op + s + len, 0u);
+                ++oi;
+                s += len;
+            }
             op += c[j];
-            oi += brick_items(c[j], a);
         }
     }
     if (threadIdx.x == kScanThreads - 1u) {
         a.offsets[a.bricks] = warp_p[kWarps - 1];
         a.items[a.bricks] = warp_i[kWarps - 1];
+        *a.next = 0u;
     }
 }
 
 // Each block histograms its particles' bricks in shared memory and adds the
 // histogram to the counts.
+// Each thread's particles in the count and scatter passes: their loads are
+// issued together before any is used, so a thread waits for memory once, not
+// once per particle.
+constexpr uint32_t kPerThread = kBrickParticlesPerBlock / kBrickBlock;
+static_assert(kBrickParticlesPerBlock % kBrickBlock == 0, "count/scatter ranges split evenly over a block");
+
 __global__ void __launch_bounds__(kBrickBlock) brick_count_kernel(BrickArgs a) {
     extern __shared__ uint32_t hist[];
+    const uint32_t first = blockIdx.x * kBrickParticlesPerBlock + threadIdx.x;
+    float4 p[kPerThread];
+#pragma unroll
+    for (uint32_t j = 0; j < kPerThread; ++j) {
+        const uint32_t i = first + j * kBrickBlock;
+        if (i < a.u.particleCount) p[j] = a.pos[i];
+    }
     for (uint32_t b = threadIdx.x; b < a.bricks; b += blockDim.x) hist[b] = 0u;
     __syncthreads();
-    const uint32_t begin = blockIdx.x * kBrickParticlesPerBlock;
-    const uint32_t end = min(begin + kBrickParticlesPerBlock, a.u.particleCount);
-    for (uint32_t i = begin + threadIdx.x; i < end; i += blockDim.x) {
+#pragma unroll
+    for (uint32_t j = 0; j < kPerThread; ++j) {
+        const uint32_t i = first + j * kBrickBlock;
+        if (i >= a.u.particleCount) break;
         Footprint f;
         uint32_t key = kOutside;
-        if (footprint(a.pos[i], a.u, f)) {
+        if (footprint(p[j], a.u, f)) {
             key = brick_of(f, a);
             atomicAdd(&hist[key], 1u);
         }
@@ -277,37 +306,29 @@ __global__ void __launch_bounds__(kBrickBlock) brick_count_kernel(BrickArgs a) {
 
 __global__ void __launch_bounds__(kBrickBlock) brick_scatter_kernel(BrickArgs a) {
     extern __shared__ uint32_t hist[];
+    const uint32_t first = blockIdx.x * kBrickParticlesPerBlock + threadIdx.x;
+    uint32_t key[kPerThread];
+#pragma unroll
+    for (uint32_t j = 0; j < kPerThread; ++j) {
+        const uint32_t i = first + j * kBrickBlock;
+        key[j] = i < a.u.particleCount ? a.keys[i] : kOutside;
+    }
     for (uint32_t b = threadIdx.x; b < a.bricks; b += blockDim.x) hist[b] = 0u;
     __syncthreads();
-    const uint32_t begin = blockIdx.x * kBrickParticlesPerBlock;
-    const uint32_t end = min(begin + kBrickParticlesPerBlock, a.u.particleCount);
-    for (uint32_t i = begin + threadIdx.x; i < end; i += blockDim.x) {
-        const uint32_t key = a.keys[i];
-        if (key < a.bricks) atomicAdd(&hist[key], 1u);
-    }
+#pragma unroll
+    for (uint32_t j = 0; j < kPerThread; ++j)
+        if (key[j] < a.bricks) atomicAdd(&hist[key[j]], 1u);
     __syncthreads();
     // This block's range of every brick it touches, then a shared cursor.
     for (uint32_t b = threadIdx.x; b < a.bricks; b += blockDim.x)
         if (hist[b]) hist[b] = atomicAdd(&a.cursor[b], hist[b]);
     __syncthreads();
-    for (uint32_t i = begin + threadIdx.x; i < end; i += blockDim.x) {
-        const uint32_t key = a.keys[i];
-        if (key >= a.bricks) continue;
-        const uint32_t slot = atomicAdd(&hist[key], 1u);
-        if (slot < a.u.particleCount) a.sorted[slot] = i;  // always: the counts came from the same keys
+#pragma unroll
+    for (uint32_t j = 0; j < kPerThread; ++j) {
+        if (key[j] >= a.bricks) continue;
+        const uint32_t slot = atomicAdd(&hist[key[j]], 1u);
+        if (slot < a.u.particleCount) a.sorted[slot] = first + j * kBrickBlock;  // always: the counts came from the same keys
     }
-}
-
-// Work item -> brick: the last b with items[b] <= item (items is
-// non-decreasing, items[0] = 0).
-__device__ __forceinline__ uint32_t item_brick(const uint32_t* items, uint32_t bricks, uint32_t item) {
-    uint32_t lo = 0, hi = bricks;  // invariant: items[lo] <= item < items[hi]
-    while (hi - lo > 1u) {
-        uint32_t mid = (lo + hi) >> 1;
-        if (items[mid] <= item) lo = mid;
-        else hi = mid;
-    }
-    return lo;
 }
 
 // Words per record in the deposit's shared tile: the six sums and one pad
@@ -320,67 +341,131 @@ constexpr uint32_t kTileStride = 7;
 // takes 138 KB of shared memory, so one block fills an SM: it gets 1024 threads to keep enough
 // shared atomics in flight; the smaller tiles fit several 256-thread blocks.
 template <uint32_t B> constexpr uint32_t deposit_threads() { return B == 16u ? 1024u : kBrickBlock; }
+// Resident blocks asked of the compiler: 64 registers a thread at most.
+template <uint32_t B> constexpr uint32_t deposit_min_blocks() { return B == 16u ? 1u : 4u; }
 
+// Persistent deposit: as many blocks as fit on the device at once, each
+// zeroing its tile once and then taking work items from a counter until none
+// is left. Per item:
+//   deposit  the chunk's particles added into the tile with shared atomics,
+//            and the y and z range of their low corners kept (warp minimum
+//            and maximum, one shared atomic per warp);
+//   flush    the tile rows inside that range (a row is T cells along x, 6 T
+//            words, contiguous in the sums as well), one warp per row: each
+//            non-zero word is added to the sums with one global atomic and
+//            zeroed again in the tile, so the next item finds a zero tile.
+// Cells outside the range hold no deposit: a particle's corners lie at its
+// low corner or one voxel above it on each axis.
 template <uint32_t B>
-__global__ void __launch_bounds__(deposit_threads<B>()) brick_deposit_kernel(BrickArgs a) {
+__global__ void __launch_bounds__(deposit_threads<B>(), deposit_min_blocks<B>()) brick_deposit_kernel(BrickArgs a) {
     constexpr uint32_t T = B + 1;
     constexpr uint32_t kCells = T * T * T;
+    constexpr uint32_t kRowWords = 6u * T;
+    constexpr uint32_t kRowSteps = (kRowWords + 31u) / 32u;
     extern __shared__ uint32_t tile[];
-    const uint32_t item = blockIdx.x;
-    if (item >= a.items[a.bricks]) return;
-    const uint32_t b = item_brick(a.items, a.bricks, item);
-    const uint32_t j = item - a.items[b];
-    const uint32_t begin = a.offsets[b] + j * a.chunk;
-    const uint32_t end = min(begin + a.chunk, a.offsets[b + 1]);
-    const uint32_t bx = b % a.per_axis, by = (b / a.per_axis) % a.per_axis, bz = b / (a.per_axis * a.per_axis);
-    const int ox = (int)(bx * B), oy = (int)(by * B), oz = (int)(bz * B);
+    __shared__ uint4 job;
+    __shared__ uint32_t range[4];  // low corners' y min, y max, z min, z max in the tile
     for (uint32_t w = threadIdx.x; w < kCells * kTileStride; w += blockDim.x) tile[w] = 0u;
-    __syncthreads();
-    // kGather particles per thread per pass: their slots, then their
-    // positions and velocities, are loaded before any is deposited, so the
-    // random gathers overlap instead of following one another.
-    constexpr uint32_t kGather = 4;
-    for (uint32_t k0 = begin + threadIdx.x; k0 < end; k0 += kGather * blockDim.x) {
-        uint32_t idx[kGather];
-        float4 pos[kGather], vel[kGather];
-#pragma unroll
-        for (uint32_t j = 0; j < kGather; ++j) {
-            const uint32_t k = k0 + j * blockDim.x;
-            idx[j] = k < end ? a.sorted[k] : kOutside;
-        }
-#pragma unroll
-        for (uint32_t j = 0; j < kGather; ++j) {
-            if (idx[j] == kOutside) continue;
-            pos[j] = a.pos[idx[j]];
-            vel[j] = a.vel[idx[j]];
-        }
-#pragma unroll
-        for (uint32_t j = 0; j < kGather; ++j) {
-            if (idx[j] == kOutside) continue;
-            Footprint f;
-            // Always inside and in this brick (the count pass put it here);
-            // the test keeps every tile index in bounds regardless.
-            if (!footprint(pos[j], a.u, f)) continue;
-            if ((uint32_t)(f.lx - ox) >= B || (uint32_t)(f.ly - oy) >= B || (uint32_t)(f.lz - oz) >= B) continue;
-            const float4 v = vel[j];
-            for_each_corner(f, a.u, a.first_index + idx[j], [&](int x, int y, int z, float w) {
-                Deposit d = deposit_values(w, f.energy, f.relative, v.x, v.y, v.z);
-                uint32_t* rec =
-                    tile + kTileStride * (((uint32_t)(z - oz) * T + (uint32_t)(y - oy)) * T + (uint32_t)(x - ox));
-#pragma unroll
-                for (int c = 0; c < 6; ++c) atomicAdd(rec + c, d.w[c]);
-            });
-        }
-    }
-    __syncthreads();
+    const uint32_t total = min(a.items[a.bricks], a.max_items);
+    const uint32_t lane = threadIdx.x & 31u, warp = threadIdx.x >> 5, warps = blockDim.x >> 5;
     const uint32_t n = a.u.volumeSize;
-    for (uint32_t w = threadIdx.x; w < kCells * 6u; w += blockDim.x) {
-        const uint32_t cell = w / 6u, c = w - cell * 6u;
-        const uint32_t val = tile[cell * kTileStride + c];
-        if (!val) continue;
-        const uint32_t tx = cell % T, ty = (cell / T) % T, tz = cell / (T * T);
-        const uint32_t x = (uint32_t)ox + tx, y = (uint32_t)oy + ty, z = (uint32_t)oz + tz;
-        if (x < n && y < n && z < n) atomicAdd(a.sums + 6ull * ((z * n + y) * n + x) + c, val);
+    // Every pass takes one counter value, so a block makes at most total + 1.
+    for (uint32_t pass = 0; pass <= total; ++pass) {
+        if (threadIdx.x == 0) {
+            const uint32_t k = atomicAdd(a.next, 1u);
+            job = k < total ? a.work[k] : make_uint4(kOutside, 0u, 0u, 0u);
+            range[0] = range[2] = B;
+            range[1] = range[3] = 0u;
+        }
+        __syncthreads();  // also puts the previous item's flush before this item's adds
+        const uint4 item = job;
+        if (item.x >= a.bricks) break;  // no work left: the same for every thread
+        const uint32_t b = item.x, begin = item.y, end = item.z;
+        const uint32_t bx = b % a.per_axis, by = (b / a.per_axis) % a.per_axis, bz = b / (a.per_axis * a.per_axis);
+        const int ox = (int)(bx * B), oy = (int)(by * B), oz = (int)(bz * B);
+        uint32_t ylo = B, yhi = 0u, zlo = B, zhi = 0u;
+        // One particle per thread per pass. Loading four before depositing
+        // any (to overlap their gathers) ran slower: 257 against 232 us for
+        // 4M particles into 16^3 bricks of a 256^3 grid, 86 against 82 us
+        // for 1M into 8^3 bricks of 128^3.
+        for (uint32_t k = begin + threadIdx.x; k < end; k += blockDim.x) {
+            const uint32_t slot = a.sorted[k];
+            const float4 p = a.pos[slot];
+            Footprint f;
+            // Always inside and in this brick (the count pass put it
+            // here); the test keeps every tile index in bounds regardless.
+            if (!footprint(p, a.u, f)) continue;
+            const uint32_t ty = (uint32_t)(f.ly - oy), tz = (uint32_t)(f.lz - oz);
+            if ((uint32_t)(f.lx - ox) >= B || ty >= B || tz >= B) continue;
+            ylo = min(ylo, ty);
+            yhi = max(yhi, ty);
+            zlo = min(zlo, tz);
+            zhi = max(zhi, tz);
+            const float4 v = a.vel[slot];
+            if (a.u.exactDeposit != 0u) {
+                // All eight corners, their values first and then their 48
+                // adds back to back. A corner of weight 0 adds zeros, the
+                // same sums as skipping it.
+                uint32_t* low = tile + kTileStride * ((tz * T + ty) * T + (uint32_t)(f.lx - ox));
+                const uint32_t sx = kTileStride * (uint32_t)(f.hx - f.lx);
+                const uint32_t sy = kTileStride * T * (uint32_t)(f.hy - f.ly);
+                const uint32_t sz = kTileStride * T * T * (uint32_t)(f.hz - f.lz);
+                Deposit d[CIC_CORNERS];
+#pragma unroll
+                for (uint32_t c = 0; c < CIC_CORNERS; ++c) {
+                    const float wx = (c & 1u) ? f.fx : 1.0f - f.fx;
+                    const float wy = (c & 2u) ? f.fy : 1.0f - f.fy;
+                    const float wz = (c & 4u) ? f.fz : 1.0f - f.fz;
+                    d[c] = deposit_values(wx * wy * wz, f.energy, f.relative, v.x, v.y, v.z);
+                }
+#pragma unroll
+                for (uint32_t c = 0; c < CIC_CORNERS; ++c) {
+                    uint32_t* rec = low + ((c & 1u) ? sx : 0u) + ((c & 2u) ? sy : 0u) + ((c & 4u) ? sz : 0u);
+#pragma unroll
+                    for (int q = 0; q < 6; ++q) atomicAdd(rec + q, d[c].w[q]);
+                }
+            } else {
+                for_each_corner(f, a.u, a.first_index + slot, [&](int x, int y, int z, float w) {
+                    Deposit d = deposit_values(w, f.energy, f.relative, v.x, v.y, v.z);
+                    uint32_t* rec = tile + kTileStride * (((uint32_t)(z - oz) * T + (uint32_t)(y - oy)) * T +
+                                                          (uint32_t)(x - ox));
+#pragma unroll
+                    for (int q = 0; q < 6; ++q) atomicAdd(rec + q, d.w[q]);
+                });
+            }
+        }
+        ylo = __reduce_min_sync(0xffffffffu, ylo);
+        yhi = __reduce_max_sync(0xffffffffu, yhi);
+        zlo = __reduce_min_sync(0xffffffffu, zlo);
+        zhi = __reduce_max_sync(0xffffffffu, zhi);
+        if (lane == 0u) {
+            atomicMin(&range[0], ylo);
+            atomicMax(&range[1], yhi);
+            atomicMin(&range[2], zlo);
+            atomicMax(&range[3], zhi);
+        }
+        __syncthreads();
+        const uint32_t y0 = range[0], z0 = range[2];
+        const uint32_t rows_y = range[1] >= y0 ? range[1] + 2u - y0 : 0u;  // low rows and the row above the last
+        const uint32_t rows_z = range[3] >= z0 ? range[3] + 2u - z0 : 0u;
+        for (uint32_t r = warp; r < rows_y * rows_z; r += warps) {
+            const uint32_t ry = y0 + r % rows_y, rz = z0 + r / rows_y;
+            const uint32_t y = (uint32_t)oy + ry, z = (uint32_t)oz + rz;
+            uint32_t* row = tile + kTileStride * ((rz * T + ry) * T);
+            uint32_t* dst = a.sums + 6ull * (((uint64_t)z * n + y) * n + (uint32_t)ox);
+#pragma unroll
+            for (uint32_t s = 0; s < kRowSteps; ++s) {
+                const uint32_t w = lane + 32u * s;
+                if (w >= kRowWords) break;
+                const uint32_t cx = w / 6u, c = w - cx * 6u;
+                uint32_t* word = row + kTileStride * cx + c;
+                const uint32_t val = *word;
+                if (val == 0u) continue;
+                *word = 0u;
+                if ((uint32_t)ox + cx < n && y < n && z < n) atomicAdd(dst + w, val);
+            }
+        }
+        __syncthreads();
     }
 }
 
@@ -502,7 +587,7 @@ static int check_shape(const gg_volume* vol, uint32_t edge, uint32_t chunk) {
 // once per device.
 static int allow_shared(const void* kernel, int bytes, int device, int slot) {
     static std::mutex mu;
-    static int done[64][4] = {};
+    static int done[64][5] = {};
     if (bytes <= 48 * 1024 || device >= 64) return GG_OK;
     std::lock_guard<std::mutex> lock(mu);
     if (done[device][slot] >= bytes) return GG_OK;
@@ -512,6 +597,32 @@ static int allow_shared(const void* kernel, int bytes, int device, int slot) {
 }
 
 static uint64_t align256(uint64_t x) { return (x + 255u) & ~255ull; }
+
+// The persistent deposit's grid: the blocks of brick_deposit_kernel<B> that
+// are resident at once on the device (its occupancy with its tile, found
+// once per device), at most one per work item.
+template <uint32_t B> static int launch_deposit(gg_context* ctx, const BrickArgs& a) {
+    constexpr int kSlot = B == 4u ? 0 : B == 8u ? 1 : 2;
+    static std::mutex mu;
+    static int resident[64][3] = {};
+    const int smem = (int)tile_bytes<B>();
+    const void* kernel = (const void*)brick_deposit_kernel<B>;
+    GG_CHECK(allow_shared(kernel, smem, ctx->device, 2 + kSlot));
+    int per_sm = 0;
+    {
+        std::lock_guard<std::mutex> lock(mu);
+        if (ctx->device < 64) per_sm = resident[ctx->device][kSlot];
+        if (per_sm == 0) {
+            GG_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, (int)deposit_threads<B>(), smem),
+                    "deposit occupancy");
+            if (per_sm < 1) per_sm = 1;
+            if (ctx->device < 64) resident[ctx->device][kSlot] = per_sm;
+        }
+    }
+    const uint64_t grid = std::min<uint64_t>(a.max_items, (uint64_t)per_sm * (uint64_t)ctx->sm_count);
+    brick_deposit_kernel<B><<<(uint32_t)std::max<uint64_t>(grid, 1u), deposit_threads<B>(), smem, ctx->stream>>>(a);
+    return GG_OK;
+}
 
 // gg_splat_bin with an explicit shape (caller holds the context lock and has
 // checked the arguments).
@@ -530,7 +641,11 @@ static int splat_bin_shaped(gg_particles* ps, gg_volume* vol, const SplatUniform
     // sorted slots, keys.
     const uint64_t counts_bytes = align256(4ull * kMaxBricks);
     const uint64_t words = counts_bytes + align256(4ull * bricks) + align256(4ull * (bricks + 1u)) * 2u;
-    const uint64_t bytes = words + 2u * align256(4ull * ps->count);
+    // Work items number at most ceil(count / chunk) + one per non-empty brick.
+    const uint64_t max_items = ((uint64_t)ps->count + chunk - 1u) / chunk + bricks;
+    if (max_items >= 0xFFFFFFFFull) return gg::fail(GG_ERR_INVALID_ARGUMENT, "Too many splat work items.");
+    const uint64_t tail = words + 2u * align256(4ull * ps->count);  // work table, then the work counter
+    const uint64_t bytes = tail + align256(16ull * max_items) + 256u;
     const uint64_t capacity_before = vol->brick_scratch_capacity;  // changes when the scratch is reallocated
     GG_CHECK(gg::ensure_capacity(ctx, &vol->brick_scratch, &vol->brick_scratch_capacity, bytes, "splat bricks"));
     char* base = static_cast<char*>(vol->brick_scratch);
@@ -545,6 +660,7 @@ static int splat_bin_shaped(gg_particles* ps, gg_volume* vol, const SplatUniform
     a.u = *u;
     a.first_index = ps->first_index;
     a.edge = edge;
+    a.edge_shift = edge == 4u ? 2u : edge == 8u ? 3u : 4u;  // check_shape admits 4, 8 and 16
     a.per_axis = per;
     a.bricks = bricks;
     a.chunk = chunk;
@@ -558,6 +674,9 @@ static int splat_bin_shaped(gg_particles* ps, gg_volume* vol, const SplatUniform
     a.items = reinterpret_cast<uint32_t*>(base + counts_bytes + align256(4ull * bricks) + align256(4ull * (bricks + 1u)));
     a.sorted = reinterpret_cast<uint32_t*>(base + words);
     a.keys = reinterpret_cast<uint32_t*>(base + words + align256(4ull * ps->count));
+    a.work = reinterpret_cast<uint4*>(base + tail);
+    a.max_items = (uint32_t)max_items;
+    a.next = reinterpret_cast<uint32_t*>(base + tail + align256(16ull * max_items));
     const int hist = (int)(4u * bricks);
     GG_CHECK(allow_shared((const void*)brick_count_kernel, hist, ctx->device, 0));
     GG_CHECK(allow_shared((const void*)brick_scatter_kernel, hist, ctx->device, 1));
@@ -571,16 +690,9 @@ static int splat_bin_shaped(gg_particles* ps, gg_volume* vol, const SplatUniform
     vol->brick_counts_zero = true;
     brick_scatter_kernel<<<blocks, kBrickBlock, hist, ctx->stream>>>(a);
     GG_CHECK(gg::launch_status("brick scatter"));
-    // Work items number at most count / chunk + one per non-empty brick.
-    const uint32_t grid = (ps->count + chunk - 1u) / chunk + bricks;
-    if (edge == 4u) {
-        brick_deposit_kernel<4><<<grid, deposit_threads<4>(), tile_bytes<4>(), ctx->stream>>>(a);
-    } else if (edge == 8u) {
-        brick_deposit_kernel<8><<<grid, deposit_threads<8>(), tile_bytes<8>(), ctx->stream>>>(a);
-    } else {
-        GG_CHECK(allow_shared((const void*)brick_deposit_kernel<16>, (int)tile_bytes<16>(), ctx->device, 2));
-        brick_deposit_kernel<16><<<grid, deposit_threads<16>(), tile_bytes<16>(), ctx->stream>>>(a);
-    }
+    if (edge == 4u) GG_CHECK(launch_deposit<4>(ctx, a));
+    else if (edge == 8u) GG_CHECK(launch_deposit<8>(ctx, a));
+    else GG_CHECK(launch_deposit<16>(ctx, a));
     return gg::launch_status("brick deposit");
 }
 
@@ -615,16 +727,16 @@ GG_API int gg_volume_create(gg_context* ctx, uint32_t size, gg_volume** out) {
     gg_volume* vol = new gg_volume();
     vol->ctx = ctx;
     vol->size = size;
-    // Default shapes, from timing every shape on the presets' settled disks
+    // Default shapes, from timing the shapes on the presets' settled disks
     // (250k/96^3, 1M/128^3, 4M/256^3, uniform and concentrated): the
     // stochastic deposit (one corner per particle) is fastest with direct
-    // global atomics at every size; the exact one with 8^3 bricks up to 128^3
-    // and with 16^3 bricks above, where 8^3 bricks make a histogram too large
-    // for more than one count block per SM.
+    // global atomics at every size; the exact one with 16^3 bricks from 96^3
+    // up (41, 73 and 230 us against 45, 83 and 620 us with 8^3 bricks), in
+    // chunks of 4096, 8192 and 16384 particles, and with 8^3 bricks below.
     vol->brick_edge[0] = 0u;
     vol->brick_chunk[0] = 0u;
-    vol->brick_edge[1] = size > 128u ? 16u : 8u;
-    vol->brick_chunk[1] = size > 128u ? 16384u : 1024u;
+    vol->brick_edge[1] = size >= 96u ? 16u : 8u;
+    vol->brick_chunk[1] = size > 128u ? 16384u : size > 96u ? 8192u : size >= 96u ? 4096u : 1024u;
     int s = gg::device_alloc(ctx, sums_bytes, (void**)&vol->sums, "volume sums");
     if (s == GG_OK) s = gg::cuda_status(cudaMemsetAsync(vol->sums, 0, sums_bytes, ctx->stream), "volume clear");
     cudaChannelFormatDesc desc = cudaCreateChannelDescHalf4();
