@@ -131,13 +131,15 @@ __global__ void __launch_bounds__(256) bin_kernel(SplatArgs a) {
 // Brick-privatised splat. The grid is cut into bricks of B^3 voxels; a
 // particle belongs to the brick holding its low corner, so its eight corners
 // fall in that brick's (B+1)^3 tile. Four launches:
-//   count    each particle's brick (its key, stored) and a per-block shared
-//            histogram of keys, summed into global counts;
+//   count    each particle's brick (its key) and its place in a per-block
+//            shared histogram of keys; each block adds its histogram to the
+//            global counts with one atomic per brick, whose old value is the
+//            block's first place in that brick, so every particle's place in
+//            its brick (its rank) is stored with its key;
 //   scan     one block: brick offsets and the work items, ceil(count /
 //            chunk) chunks of each brick's sorted range, listed in a table;
-//   scatter  the histogram again from the stored keys, each block reserving
-//            its range of every brick with one atomic, then particle indices
-//            written into brick order;
+//   scatter  each particle's index written at its brick's offset plus its
+//            rank: brick order, with no atomics;
 //   deposit  persistent blocks taking work items from a counter: the tile's
 //            records (six words and a pad, see kTileStride) in shared
 //            memory, the chunk's particles deposited there with shared
@@ -147,7 +149,7 @@ __global__ void __launch_bounds__(256) bin_kernel(SplatArgs a) {
 // the direct kernel's bit for bit.
 
 constexpr uint32_t kBrickBlock = 256;
-constexpr uint32_t kBrickParticlesPerBlock = 2048;  // count/scatter range of one block
+constexpr uint32_t kBrickParticlesPerBlock = 2048;  // count range of one block
 constexpr uint32_t kOutside = 0xFFFFFFFFu;          // key of a particle outside the cube
 constexpr uint32_t kMaxBricks = 32768;               // histogram of 128 KB shared memory
 
@@ -165,10 +167,10 @@ struct BrickArgs {
     uint32_t chunk_shift;  // log2(chunk) when chunk is a power of two, else 32
     uint32_t* counts;    // [kMaxBricks], zero between calls (the scan re-zeroes what it read)
     uint32_t* offsets;   // [bricks + 1], exclusive scan of counts
-    uint32_t* cursor;    // [bricks], reservation cursor
     uint32_t* items;     // [bricks + 1], exclusive scan of ceil(count / chunk)
     uint32_t* sorted;    // [particleCount], particle slots in brick order
     uint32_t* keys;      // [particleCount], each particle's brick (kOutside: none), from the count pass
+    uint32_t* ranks;     // [particleCount], each particle's place in its brick, from the count pass
     uint4* work;         // [max_items], per work item: brick, first and end sorted slot (from the scan)
     uint32_t max_items;  // ceil(particleCount / chunk) + bricks, a bound on the work items
     uint32_t* next;      // the deposit blocks' work counter (zeroed by the scan)
@@ -195,7 +197,7 @@ __device__ __forceinline__ uint32_t brick_items(uint32_t c, const BrickArgs& a) 
     return a.chunk_shift < 32u ? (c + a.chunk - 1u) >> a.chunk_shift : (c + a.chunk - 1u) / a.chunk;
 }
 
-// Exclusive scans of the brick counts (offsets, cursor) and of their work
+// Exclusive scans of the brick counts (offsets) and of their work
 // items (items), by one block of kScanThreads threads: each thread scans a
 // contiguous run of bricks, loading its counts kScanBatch at a time so the
 // loads are in flight together; the per-thread totals are scanned with warp
@@ -249,7 +251,6 @@ __global__ void __launch_bounds__(kScanThreads) brick_scan_kernel(BrickArgs a) {
             if (b + j >= b1) break;
             a.counts[b + j] = 0u;
             a.offsets[b + j] = op;
-            a.cursor[b + j] = op;
             a.items[b + j] = oi;
             // The brick's work items: consecutive chunks of its sorted range.
             for (uint32_t s = 0; s < c[j];) {
@@ -270,11 +271,11 @@ __global__ void __launch_bounds__(kScanThreads) brick_scan_kernel(BrickArgs a) {
 
 // Each block histograms its particles' bricks in shared memory and adds the
 // histogram to the counts.
-// Each thread's particles in the count and scatter passes: their loads are
-// issued together before any is used, so a thread waits for memory once, not
-// once per particle.
+// Each thread's particles in the count pass: their loads are issued
+// together before any is used, so a thread waits for memory once, not once
+// per particle.
 constexpr uint32_t kPerThread = kBrickParticlesPerBlock / kBrickBlock;
-static_assert(kBrickParticlesPerBlock % kBrickBlock == 0, "count/scatter ranges split evenly over a block");
+static_assert(kBrickParticlesPerBlock % kBrickBlock == 0, "count ranges split evenly over a block");
 
 __global__ void __launch_bounds__(kBrickBlock) brick_count_kernel(BrickArgs a) {
     extern __shared__ uint32_t hist[];
@@ -287,48 +288,40 @@ __global__ void __launch_bounds__(kBrickBlock) brick_count_kernel(BrickArgs a) {
     }
     for (uint32_t b = threadIdx.x; b < a.bricks; b += blockDim.x) hist[b] = 0u;
     __syncthreads();
+    uint32_t key[kPerThread], rank[kPerThread];
+#pragma unroll
+    for (uint32_t j = 0; j < kPerThread; ++j) {
+        key[j] = kOutside;
+        rank[j] = 0u;
+        Footprint f;
+        if (first + j * kBrickBlock < a.u.particleCount && footprint(p[j], a.u, f)) {
+            key[j] = brick_of(f, a);
+            rank[j] = atomicAdd(&hist[key[j]], 1u);  // place among this block's particles of the brick
+        }
+    }
+    __syncthreads();
+    // The block's histogram into the counts; each old count is where the
+    // block's particles of that brick start.
+    for (uint32_t b = threadIdx.x; b < a.bricks; b += blockDim.x)
+        if (hist[b]) hist[b] = atomicAdd(&a.counts[b], hist[b]);
+    __syncthreads();
 #pragma unroll
     for (uint32_t j = 0; j < kPerThread; ++j) {
         const uint32_t i = first + j * kBrickBlock;
         if (i >= a.u.particleCount) break;
-        Footprint f;
-        uint32_t key = kOutside;
-        if (footprint(p[j], a.u, f)) {
-            key = brick_of(f, a);
-            atomicAdd(&hist[key], 1u);
-        }
-        a.keys[i] = key;
+        a.keys[i] = key[j];
+        if (key[j] != kOutside) a.ranks[i] = hist[key[j]] + rank[j];
     }
-    __syncthreads();
-    for (uint32_t b = threadIdx.x; b < a.bricks; b += blockDim.x)
-        if (hist[b]) atomicAdd(&a.counts[b], hist[b]);
 }
 
+// One particle per thread: its index at its brick's offset plus its rank.
 __global__ void __launch_bounds__(kBrickBlock) brick_scatter_kernel(BrickArgs a) {
-    extern __shared__ uint32_t hist[];
-    const uint32_t first = blockIdx.x * kBrickParticlesPerBlock + threadIdx.x;
-    uint32_t key[kPerThread];
-#pragma unroll
-    for (uint32_t j = 0; j < kPerThread; ++j) {
-        const uint32_t i = first + j * kBrickBlock;
-        key[j] = i < a.u.particleCount ? a.keys[i] : kOutside;
-    }
-    for (uint32_t b = threadIdx.x; b < a.bricks; b += blockDim.x) hist[b] = 0u;
-    __syncthreads();
-#pragma unroll
-    for (uint32_t j = 0; j < kPerThread; ++j)
-        if (key[j] < a.bricks) atomicAdd(&hist[key[j]], 1u);
-    __syncthreads();
-    // This block's range of every brick it touches, then a shared cursor.
-    for (uint32_t b = threadIdx.x; b < a.bricks; b += blockDim.x)
-        if (hist[b]) hist[b] = atomicAdd(&a.cursor[b], hist[b]);
-    __syncthreads();
-#pragma unroll
-    for (uint32_t j = 0; j < kPerThread; ++j) {
-        if (key[j] >= a.bricks) continue;
-        const uint32_t slot = atomicAdd(&hist[key[j]], 1u);
-        if (slot < a.u.particleCount) a.sorted[slot] = first + j * kBrickBlock;  // always: the counts came from the same keys
-    }
+    const uint32_t i = blockIdx.x * kBrickBlock + threadIdx.x;
+    if (i >= a.u.particleCount) return;
+    const uint32_t key = a.keys[i];
+    if (key >= a.bricks) return;
+    const uint32_t slot = a.offsets[key] + a.ranks[i];
+    if (slot < a.u.particleCount) a.sorted[slot] = i;  // always: ranks and offsets came from the same counts
 }
 
 // Words per record in the deposit's shared tile: the six sums and one pad
@@ -637,14 +630,14 @@ static int splat_bin_shaped(gg_particles* ps, gg_volume* vol, const SplatUniform
     const uint32_t per = bricks_per_axis(vol->size, edge);
     const uint32_t bricks = per * per * per;
     // counts (a fixed kMaxBricks words, whatever the shape, so that the
-    // zeros the scan leaves behind stay counts), cursor, offsets, items,
-    // sorted slots, keys.
+    // zeros the scan leaves behind stay counts), offsets, items, sorted
+    // slots, keys, ranks.
     const uint64_t counts_bytes = align256(4ull * kMaxBricks);
-    const uint64_t words = counts_bytes + align256(4ull * bricks) + align256(4ull * (bricks + 1u)) * 2u;
+    const uint64_t words = counts_bytes + align256(4ull * (bricks + 1u)) * 2u;
     // Work items number at most ceil(count / chunk) + one per non-empty brick.
     const uint64_t max_items = ((uint64_t)ps->count + chunk - 1u) / chunk + bricks;
     if (max_items >= 0xFFFFFFFFull) return gg::fail(GG_ERR_INVALID_ARGUMENT, "Too many splat work items.");
-    const uint64_t tail = words + 2u * align256(4ull * ps->count);  // work table, then the work counter
+    const uint64_t tail = words + 3u * align256(4ull * ps->count);  // work table, then the work counter
     const uint64_t bytes = tail + align256(16ull * max_items) + 256u;
     const uint64_t capacity_before = vol->brick_scratch_capacity;  // changes when the scratch is reallocated
     GG_CHECK(gg::ensure_capacity(ctx, &vol->brick_scratch, &vol->brick_scratch_capacity, bytes, "splat bricks"));
@@ -669,17 +662,16 @@ static int splat_bin_shaped(gg_particles* ps, gg_volume* vol, const SplatUniform
         for (uint32_t k = 0; k < 32u; ++k)
             if ((1u << k) == chunk) a.chunk_shift = k;
     a.counts = reinterpret_cast<uint32_t*>(base);
-    a.cursor = reinterpret_cast<uint32_t*>(base + counts_bytes);
-    a.offsets = reinterpret_cast<uint32_t*>(base + counts_bytes + align256(4ull * bricks));
-    a.items = reinterpret_cast<uint32_t*>(base + counts_bytes + align256(4ull * bricks) + align256(4ull * (bricks + 1u)));
+    a.offsets = reinterpret_cast<uint32_t*>(base + counts_bytes);
+    a.items = reinterpret_cast<uint32_t*>(base + counts_bytes + align256(4ull * (bricks + 1u)));
     a.sorted = reinterpret_cast<uint32_t*>(base + words);
     a.keys = reinterpret_cast<uint32_t*>(base + words + align256(4ull * ps->count));
+    a.ranks = reinterpret_cast<uint32_t*>(base + words + 2u * align256(4ull * ps->count));
     a.work = reinterpret_cast<uint4*>(base + tail);
     a.max_items = (uint32_t)max_items;
     a.next = reinterpret_cast<uint32_t*>(base + tail + align256(16ull * max_items));
     const int hist = (int)(4u * bricks);
     GG_CHECK(allow_shared((const void*)brick_count_kernel, hist, ctx->device, 0));
-    GG_CHECK(allow_shared((const void*)brick_scatter_kernel, hist, ctx->device, 1));
     const uint32_t blocks = (ps->count + kBrickParticlesPerBlock - 1u) / kBrickParticlesPerBlock;
     // A failed launch leaves the counts in an unknown state: clear them next time.
     vol->brick_counts_zero = false;
@@ -688,7 +680,7 @@ static int splat_bin_shaped(gg_particles* ps, gg_volume* vol, const SplatUniform
     brick_scan_kernel<<<1, kScanThreads, 0, ctx->stream>>>(a);
     GG_CHECK(gg::launch_status("brick scan"));
     vol->brick_counts_zero = true;
-    brick_scatter_kernel<<<blocks, kBrickBlock, hist, ctx->stream>>>(a);
+    brick_scatter_kernel<<<(ps->count + kBrickBlock - 1u) / kBrickBlock, kBrickBlock, 0, ctx->stream>>>(a);
     GG_CHECK(gg::launch_status("brick scatter"));
     if (edge == 4u) GG_CHECK(launch_deposit<4>(ctx, a));
     else if (edge == 8u) GG_CHECK(launch_deposit<8>(ctx, a));
