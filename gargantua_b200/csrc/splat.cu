@@ -533,7 +533,10 @@ __device__ __forceinline__ float resolve_inverse_volume(const ResolveArgs& a) {
 // neighbouring rows. Against 128 voxels of one row per block this ran the
 // 256^3 resolve in 203 us instead of 252 (the surface stores of a block land
 // in fewer tiles of the block-linear texture layout); four voxels per thread
-// were slower at 128^3 (fewer waves of blocks) and no faster at 256^3.
+// were slower at 128^3 (fewer waves of blocks) and no faster at 256^3, and
+// two neighbouring voxels per thread with 16-byte record loads and clearing
+// stores slower at both (38.6 against 30.9 us at 128^3, 255 against 210 at
+// 256^3).
 constexpr uint32_t kResolveRows = 8;
 
 __global__ void __launch_bounds__(32 * kResolveRows) resolve_kernel(ResolveArgs a) {
