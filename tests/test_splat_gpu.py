@@ -119,7 +119,7 @@ def test_size_mismatch_is_an_argument_error(ctx, settled):
     assert status == 1
 
 
-SHAPES = [(0, 0), (4, 1024), (8, 64), (8, 2048), (16, 4096), (16, 100000)]
+SHAPES = [(0, 0), (4, 1024), (8, 64), (8, 1000), (8, 2048), (16, 3), (16, 4096), (16, 100000)]
 
 
 @pytest.mark.parametrize("shape", SHAPES, ids=[f"edge{e}-chunk{c}" for e, c in SHAPES])
@@ -127,7 +127,9 @@ SHAPES = [(0, 0), (4, 1024), (8, 64), (8, 2048), (16, 4096), (16, 100000)]
 @pytest.mark.parametrize("exact", [True, False])
 def test_every_splat_shape_is_bit_exact(ctx, settled, shape, size, exact):
     """Direct atomics and the brick-privatised deposit (ragged last bricks at
-    100^3, many work items per brick at chunk 64) give the replica's grids."""
+    100^3, many work items per brick at chunk 64, a chunk that is not a power
+    of two, and chunk 3: over 20,000 work items taken by the persistent
+    deposit blocks) give the replica's grids."""
     import gargantua_b200 as g
 
     vol = g.Volume(ctx, size)
@@ -160,6 +162,29 @@ def test_crowded_voxels_are_bit_exact(ctx, exact):
         rem, rmo, rma = O.deposit32(ps.read(), 48, frame=3, exact=exact, seed=7)
         assert ma.max() > 256 * 100  # some voxel holds the mass of over a hundred particles
         assert np.array_equal(em, rem) and np.array_equal(mo, rmo) and np.array_equal(ma, rma), (edge, chunk)
+    vol.close()
+    ps.close()
+
+
+@pytest.mark.parametrize("exact", [True, False])
+def test_particles_all_outside_leave_the_grid_empty(ctx, exact):
+    """No particle inside the cube: the count pass keys none, the scan lists
+    no work item, and every brick shape leaves the sums at zero."""
+    import gargantua_b200 as g
+
+    n = 5000
+    parts = np.zeros((n, 8), np.float32)
+    rng = np.random.default_rng(3)
+    parts[:, :3] = rng.uniform(31.0, 50.0, (n, 3)).astype(np.float32) * rng.choice([-1.0, 1.0], (n, 3))
+    parts[:, 3] = 1.0
+    ps = g.Particles(ctx, n, seed=1)
+    ps.write(parts)
+    vol = g.Volume(ctx, 64)
+    for edge, chunk in [(0, 0), (4, 1024), (8, 64), (16, 4096)]:
+        vol.set_shape(exact, edge, chunk)
+        vol.bin(ps, exact=exact, frame=1)
+        em, mo, ma = vol.read_sums()
+        assert not em.any() and not mo.any() and not ma.any(), (edge, chunk)
     vol.close()
     ps.close()
 
