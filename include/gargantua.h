@@ -186,8 +186,9 @@ GG_API int gg_volume_write_sums(gg_volume* vol, const uint32_t* emission, const 
  * is cut into bricks of that edge, particles are sorted by brick, and each
  * work item of `chunk` particles of one brick deposits into a shared-memory
  * copy of its (edge+1)^3 voxels before adding the non-zero words to the
- * sums. Every shape gives the same sums bit for bit. Default: edge 8, chunk
- * 2048 (exact) and 4096 (stochastic). */
+ * sums. Every shape gives the same sums bit for bit. Defaults: exact, edge
+ * 16 with chunks of 4096 (96^3), 8192 (up to 128^3) and 16384 particles
+ * (larger), edge 8 with chunks of 1024 below 96^3; stochastic, edge 0. */
 GG_API int gg_volume_splat_shape(gg_volume* vol, int exact, uint32_t brick_edge, uint32_t chunk);
 
 /* Time gg_splat_bin under each shape on these particles (u->exactDeposit
