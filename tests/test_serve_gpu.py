@@ -37,6 +37,10 @@ def mix_specs():
         g.RequestSpec(480, 270, 4096, 0.5, azimuth=2.0, elevation=1.2, distance=45.0),
         g.RequestSpec(320, 180, 256, 0.0, azimuth=-0.4, elevation=0.2, distance=110.0),
         g.RequestSpec(160, 90, 4096, 0.9, azimuth=0.2, elevation=0.1, distance=40.0),
+        # The ends of the spin range (Options.swift:119-124): near-extremal,
+        # and barely spinning (the Kerr path, not the Schwarzschild one).
+        g.RequestSpec(240, 135, 4096, 0.998, azimuth=0.9, elevation=0.3, distance=50.0),
+        g.RequestSpec(240, 135, 256, 0.02, azimuth=3.0, elevation=0.7, distance=60.0),
     ]
 
 
