@@ -64,6 +64,25 @@ def test_step_is_bit_exact_against_the_replica_over_1000_substeps(ctx):
     assert ps.checksum() == O.fnv1a(ref)
 
 
+def test_newtonian_potential_is_bit_exact_against_the_replica(ctx):
+    """The second potential of Common.h:32-46 (g = 1/r^2): seed and 1000
+    substeps bit-exact against the replica. (The weaker pull plunges few
+    particles in that time; the respawn path is covered above.)"""
+    import gargantua_b200 as g
+
+    n = 20000
+    ps = g.Particles(ctx, n, seed=9, potential=g.types.POTENTIAL_NEWTONIAN)
+    ps.seed_particles()
+    ps.step(500)
+    dev = ps.read()
+    u, cdf = replica_args(ps)
+    ref = O.seed32(n, 9, g.types.POTENTIAL_NEWTONIAN, cdf, u.temperatureScale)
+    O.step32(ref, 9, g.types.POTENTIAL_NEWTONIAN, cdf, u.dt, u.alpha, u.temperatureScale, 500)
+    mismatch = np.flatnonzero((dev.view(np.uint32) != ref.view(np.uint32)).any(axis=1))
+    assert mismatch.size == 0, f"{mismatch.size} particles differ, first {mismatch[:5]}"
+    assert ps.checksum() == O.fnv1a(ref)
+
+
 def test_step_from_arbitrary_state_matches_replica(ctx):
     """Edge cases: particles on the capture sphere, beyond the escape radius,
     over the speed limit and at the origin's neighbourhood, uploaded through
