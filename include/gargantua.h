@@ -402,7 +402,10 @@ GG_API int gg_write_png(const char* path, const uint8_t* rgba8, uint32_t width, 
  * policy, Schwarzschild.swift:167-172), a spin (0 renders Schwarzschild with
  * the sphere jump, > 0 Kerr) and a star seed. The server writes width*height
  * rgba16f pixels into `output` (host memory the caller keeps alive until the
- * request completes) and, when debug_output is not NULL, the debug target
+ * request completes; page-locked memory, cudaHostAlloc, copies at the link's
+ * rate: a 1920x1080 result's 16.6 MB took 0.3 ms into page-locked memory and
+ * 1.7 to 4.5 ms into pageable memory on a B200) and, when debug_output is not
+ * NULL, the debug target
  * (drift, steps, outcome, 1). Kerr cameras beyond R_ESCAPE escape at
  * camera distance + 10 instead of R_ESCAPE, so rays start inside the scene.
  * Replaces a `--still` render (Still.swift:9-99) as a served unit of work. */
