@@ -56,6 +56,8 @@ SIGNATURES = {
     "gg_context_synchronize": (i, [vp]),
     "gg_context_memory": (i, [vp, P(u64), P(u64)]),
     "gg_context_stream": (vp, [vp]),
+    "gg_host_alloc": (i, [vp, u64, P(vp)]),
+    "gg_host_free": (None, [vp]),
     "gg_context_blackbody": (i, [vp, f32p, u32]),
     "gg_particles_create": (i, [vp, u32, u64, u32, P(vp)]),
     "gg_particles_destroy": (None, [vp]),

@@ -30,6 +30,7 @@
 #include <cstdarg>
 #include <cstring>
 #include <functional>
+#include <memory>
 #include <string>
 #include <vector>
 
@@ -308,7 +309,14 @@ void still(const Options& o) {
     cfg.mode = GG_SERVE_BATCHED;
     gg_server* server = nullptr;
     check(gg_server_create(s.ctx, s.vol, &cfg, &server));
-    std::vector<uint16_t> pixels((size_t)o.width * o.height * 4);
+    // The result copies into page-locked memory at the link's rate.
+    const size_t halves = (size_t)o.width * o.height * 4;
+    void* block = nullptr;
+    int status = gg_host_alloc(s.ctx, halves * sizeof(uint16_t), &block);
+    if (status != GG_OK) gg_server_destroy(server);
+    check(status);
+    std::unique_ptr<uint16_t, void (*)(uint16_t*)> pixels(static_cast<uint16_t*>(block),
+                                                          [](uint16_t* p) { gg_host_free(p); });
     gg_request q;
     std::memset(&q, 0, sizeof q);
     q.azimuth = (float)o.azimuth;
@@ -320,11 +328,11 @@ void still(const Options& o) {
     q.step_cap = STEP_CAP_STILL;
     q.spin = (float)o.spin;
     q.star_seed = (uint32_t)o.seed;
-    q.output = pixels.data();
+    q.output = pixels.get();
     uint64_t ticket = 0;
     gg_request_result res;
     const double t0 = seconds_now();
-    int status = gg_server_submit(server, &q, &ticket);
+    status = gg_server_submit(server, &q, &ticket);
     if (status == GG_OK) status = gg_server_wait(server, ticket, 3600.0, &res);
     const double wall = seconds_now() - t0;
     uint64_t requests = 0, steps = 0, launches = 0;
@@ -340,7 +348,7 @@ void still(const Options& o) {
     print_counters(res.counters);
     gg_targets* t = nullptr;
     check(gg_targets_create(s.ctx, o.width, o.height, &t));
-    status = gg_targets_write(t, pixels.data(), nullptr);
+    status = gg_targets_write(t, pixels.get(), nullptr);
     if (status == GG_OK) {
         try {
             write_tonemapped(t, o.width, o.height, DRIFT_BUDGET_STILL, o.still_path);

@@ -272,4 +272,24 @@ GG_API int gg_context_memory(gg_context* ctx, uint64_t* budget, uint64_t* used) 
 
 GG_API void* gg_context_stream(gg_context* ctx) { return ctx ? (void*)ctx->stream : nullptr; }
 
+GG_API int gg_host_alloc(gg_context* ctx, uint64_t bytes, void** out) {
+    if (!ctx || !out) return gg::fail(GG_ERR_INVALID_ARGUMENT, "gg_host_alloc needs a context and an output.");
+    *out = nullptr;
+    if (bytes == 0) return gg::fail(GG_ERR_INVALID_ARGUMENT, "gg_host_alloc needs a positive size.");
+    std::lock_guard<std::recursive_mutex> lock(ctx->mu);
+    GG_CUDA(cudaSetDevice(ctx->device), "cudaSetDevice");
+    const cudaError_t e = cudaHostAlloc(out, (size_t)bytes, cudaHostAllocPortable);
+    if (e != cudaSuccess) {
+        *out = nullptr;
+        cudaGetLastError();
+        return gg::fail(GG_ERR_OUT_OF_MEMORY, "Page-locked host memory of %llu bytes is not available (%s).",
+                        (unsigned long long)bytes, cudaGetErrorString(e));
+    }
+    return GG_OK;
+}
+
+GG_API void gg_host_free(void* p) {
+    if (p) cudaFreeHost(p);
+}
+
 }  // extern "C"

@@ -616,6 +616,24 @@ class RequestSpec:
     volume: "Volume | None" = None  # None: the server's volume
 
 
+def pinned_array(ctx: Context, shape, dtype=np.float16) -> np.ndarray:
+    """A numpy array in page-locked host memory (gg_host_alloc): the
+    library's copies into or out of it run at the link's rate. The memory is
+    released (gg_host_free) once the array and every view of it are gone."""
+    dtype = np.dtype(dtype)
+    shape = tuple(int(x) for x in (shape if isinstance(shape, (tuple, list)) else (shape,)))
+    nbytes = int(np.prod(shape)) * dtype.itemsize
+    p = C.c_void_p()
+    check(lib().gg_host_alloc(ctx.handle, max(nbytes, 1), C.byref(p)))
+    free = lib().gg_host_free
+    address = p.value
+    # A ctypes array over the block whose finaliser frees it; numpy arrays
+    # made from it keep it alive through their base.
+    block_type = type("PinnedBlock", (C.c_char * max(nbytes, 1),), {"__del__": lambda self: free(address)})
+    block = block_type.from_address(address)
+    return np.frombuffer(block, dtype=np.uint8, count=nbytes).view(dtype).reshape(shape)
+
+
 def expect_size(a: np.ndarray, values: int, what: str) -> None:
     """The library reads or writes exactly `values` elements at an array's
     address: refuse any other size before it does."""
@@ -665,12 +683,14 @@ class Server:
 
     def submit(self, spec: RequestSpec, output: np.ndarray | None = None, debug: bool = False) -> int:
         """Queue a request; `output` (height*width*4 float16, kept alive here)
-        receives the pixels."""
+        receives the pixels. Without one, the request gets page-locked
+        arrays (pinned_array), into which the result copies at the link's
+        rate."""
         n = spec.width * spec.height
         if output is None:
-            output = np.zeros((n, 4), np.float16)
+            output = pinned_array(self.ctx, (n, 4), np.float16)
         check_pixel_buffer(output, n)
-        dbg = np.zeros((n, 4), np.float16) if debug else None
+        dbg = pinned_array(self.ctx, (n, 4), np.float16) if debug else None
         q = T.Request(spec.azimuth, spec.elevation, spec.distance, spec.fov_y, spec.width, spec.height,
                       spec.step_cap, spec.spin, spec.star_seed & 0xFFFFFFFF, spec.flags,
                       output.ctypes.data, dbg.ctypes.data if dbg is not None else None,

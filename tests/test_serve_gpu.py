@@ -96,6 +96,39 @@ def test_each_result_is_the_same_alone_and_in_the_mix(world):
     server.close()
 
 
+def test_page_locked_outputs_match_pageable_ones(world):
+    """gg_host_alloc / gg_host_free: a request served into page-locked memory
+    (Server.submit's default) gives the pixels a pageable array gets, a view
+    outlives its array, and blocks are released as their arrays go."""
+    import gc
+
+    import gargantua_b200 as g
+
+    spec = g.RequestSpec(320, 180, 256, 0.5, azimuth=0.7, elevation=0.3, distance=55.0)
+    server = g.Server(world["ctx"], world["vol"], g.types.SERVE_BATCHED)
+    pageable = np.zeros((320 * 180, 4), np.float16)
+    a = server.wait(server.submit(spec, pageable))[0]
+    b = server.wait(server.submit(spec))[0]
+    assert np.array_equal(a.view(np.uint16), b.view(np.uint16))
+    copy = b[1000:1010].copy()
+    view = b[1000:1010]
+    del b
+    gc.collect()
+    assert np.array_equal(copy.view(np.uint16), view.view(np.uint16))  # the view still reads the block
+    server.close()
+    for _ in range(64):  # 64 MB allocated and released in turn
+        block = g.pinned_array(world["ctx"], (1 << 20,), np.uint8)
+        block[:] = 7
+        assert int(block.sum()) == 7 << 20
+        del block
+    import ctypes as C
+
+    from gargantua_b200._lib import check
+
+    with pytest.raises(g.GargantuaError):  # a zero size is refused with a sentence
+        check(g.lib().gg_host_alloc(world["ctx"].handle, 0, C.byref(C.c_void_p())))
+
+
 def test_overlapping_arrivals_are_admitted_as_memory_frees(world):
     """A server whose memory holds about two requests still completes a
     stream of eight, admitting each as an earlier one releases its targets."""
