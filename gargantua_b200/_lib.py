@@ -80,6 +80,8 @@ SIGNATURES = {
     "gg_volume_read_sums": (i, [vp, vp, vp, vp]),
     "gg_volume_write_sums": (i, [vp, vp, vp, vp]),
     "gg_volume_sums": (i, [vp, P(vp), P(u64)]),
+    "gg_volume_ipc_handle": (i, [vp, vp]),
+    "gg_volume_attach_peers": (i, [vp, vp, u32]),
     "gg_volume_splat_shape": (i, [vp, i, u32, u32]),
     "gg_splat_autotune": (i, [vp, vp, P(T.SplatUniforms), P(u32), P(u32), P(C.c_float)]),
     "gg_volume_read": (i, [vp, vp, vp]),

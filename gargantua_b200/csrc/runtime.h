@@ -154,6 +154,10 @@ struct gg_volume {
     void* brick_scratch = nullptr;  // counts, cursor, offsets, items, sorted slots, keys
     uint64_t brick_scratch_capacity = 0;
     bool brick_counts_zero = false;  // the counts region holds zeros (the count pass re-zeroes it)
+    // Other ranks' sums opened from their IPC handles (gg_volume_attach_peers):
+    // every deposit word is added into each of them as well.
+    uint32_t* peer_sums[GG_MAX_PEERS] = {};
+    uint32_t peers = 0;
 };
 
 struct gg_targets {

@@ -12,6 +12,7 @@
 // are: this translation unit is built with --fmad=false and evaluates every
 // float expression in the order the CPU replica (oracle/replica.c) does.
 #include <algorithm>
+#include <cstring>
 #include <mutex>
 #include <vector>
 
@@ -26,12 +27,31 @@ constexpr float ENERGY_T_FIXED = 1048576.0f; // 2^20
 constexpr float MOMENTUM_FIXED = 4096.0f;    // 2^12
 constexpr float MASS_FIXED = 256.0f;         // 2^8
 
+// Other ranks' copies of the sums (gg_volume_attach_peers), opened from
+// their IPC handles: every word deposited here is added into each of them at
+// the same offset, so the deposit is also the all-reduce.
+struct PeerSums {
+    uint32_t* sums[GG_MAX_PEERS];
+    uint32_t count;
+};
+
+// One word into the sums and into every peer's copy.
+__device__ __forceinline__ void add_word(uint32_t* sums, const PeerSums& peers, uint64_t offset, uint32_t v) {
+    atomicAdd(sums + offset, v);
+    if (peers.count != 0u) {
+#pragma unroll
+        for (uint32_t p = 0; p < GG_MAX_PEERS; ++p)
+            if (p < peers.count) atomicAdd(peers.sums[p] + offset, v);
+    }
+}
+
 struct SplatArgs {
     const float4* __restrict__ pos;
     const float4* __restrict__ vel;
     uint32_t* __restrict__ sums;
     SplatUniforms u;
     uint32_t first_index;  // global index of slot 0, for the stochastic pick
+    PeerSums peers;
 };
 
 // A particle's cloud-in-cell footprint (splat.metal:44-70): positions mapped
@@ -110,7 +130,7 @@ __device__ __forceinline__ void for_each_corner(const Footprint& f, const SplatU
 }
 
 // splatParticles (splat.metal:44-88), one thread per particle, six global
-// atomics per corner straight into the sums.
+// atomics per corner straight into the sums (and into each peer's copy).
 __global__ void __launch_bounds__(256) bin_kernel(SplatArgs a) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     const SplatUniforms& u = a.u;
@@ -121,9 +141,9 @@ __global__ void __launch_bounds__(256) bin_kernel(SplatArgs a) {
     const uint32_t n = u.volumeSize;
     for_each_corner(f, u, a.first_index + i, [&](int x, int y, int z, float w) {
         Deposit d = deposit_values(w, f.energy, f.relative, v.x, v.y, v.z);
-        uint32_t* rec = a.sums + 6ull * (((uint32_t)z * n + (uint32_t)y) * n + (uint32_t)x);
+        const uint64_t rec = 6ull * (((uint32_t)z * n + (uint32_t)y) * n + (uint32_t)x);
 #pragma unroll
-        for (int k = 0; k < 6; ++k) atomicAdd(rec + k, d.w[k]);
+        for (int k = 0; k < 6; ++k) add_word(a.sums, a.peers, rec + k, d.w[k]);
     });
 }
 
@@ -143,8 +163,9 @@ __global__ void __launch_bounds__(256) bin_kernel(SplatArgs a) {
 //   deposit  persistent blocks taking work items from a counter: the tile's
 //            records (six words and a pad, see kTileStride) in shared
 //            memory, the chunk's particles deposited there with shared
-//            atomics, the non-zero words added to the sums with one global
-//            atomic each and zeroed for the next item.
+//            atomics, the non-zero words added to the sums (and to each
+//            peer's copy) with one global atomic each and zeroed for the
+//            next item.
 // Integer sums do not depend on the order of the adds, so the grid equals
 // the direct kernel's bit for bit.
 
@@ -174,6 +195,7 @@ struct BrickArgs {
     uint4* work;         // [max_items], per work item: brick, first and end sorted slot (from the scan)
     uint32_t max_items;  // ceil(particleCount / chunk) + bricks, a bound on the work items
     uint32_t* next;      // the deposit blocks' work counter (zeroed by the scan)
+    PeerSums peers;
 };
 
 __device__ __forceinline__ uint32_t brick_of(const Footprint& f, const BrickArgs& a) {
@@ -445,7 +467,7 @@ __global__ void __launch_bounds__(deposit_threads<B>(), deposit_min_blocks<B>())
             const uint32_t ry = y0 + r % rows_y, rz = z0 + r / rows_y;
             const uint32_t y = (uint32_t)oy + ry, z = (uint32_t)oz + rz;
             uint32_t* row = tile + kTileStride * ((rz * T + ry) * T);
-            uint32_t* dst = a.sums + 6ull * (((uint64_t)z * n + y) * n + (uint32_t)ox);
+            const uint64_t dst = 6ull * (((uint64_t)z * n + y) * n + (uint32_t)ox);
 #pragma unroll
             for (uint32_t s = 0; s < kRowSteps; ++s) {
                 const uint32_t w = lane + 32u * s;
@@ -455,7 +477,7 @@ __global__ void __launch_bounds__(deposit_threads<B>(), deposit_min_blocks<B>())
                 const uint32_t val = *word;
                 if (val == 0u) continue;
                 *word = 0u;
-                if ((uint32_t)ox + cx < n && y < n && z < n) atomicAdd(dst + w, val);
+                if ((uint32_t)ox + cx < n && y < n && z < n) add_word(a.sums, a.peers, dst + w, val);
             }
         }
         __syncthreads();
@@ -594,6 +616,20 @@ static int allow_shared(const void* kernel, int bytes, int device, int slot) {
 
 static uint64_t align256(uint64_t x) { return (x + 255u) & ~255ull; }
 
+static PeerSums peer_sums(const gg_volume* vol) {
+    PeerSums p{};
+    p.count = vol->peers;
+    for (uint32_t k = 0; k < vol->peers && k < GG_MAX_PEERS; ++k) p.sums[k] = vol->peer_sums[k];
+    return p;
+}
+
+static void close_peers(gg_volume* vol) {
+    for (uint32_t k = 0; k < vol->peers && k < GG_MAX_PEERS; ++k)
+        if (vol->peer_sums[k]) cudaIpcCloseMemHandle(vol->peer_sums[k]);
+    for (uint32_t k = 0; k < GG_MAX_PEERS; ++k) vol->peer_sums[k] = nullptr;
+    vol->peers = 0;
+}
+
 // The persistent deposit's grid: the blocks of brick_deposit_kernel<B> that
 // are resident at once on the device (its occupancy with its tile, found
 // once per device), at most one per work item.
@@ -625,7 +661,7 @@ template <uint32_t B> static int launch_deposit(gg_context* ctx, const BrickArgs
 static int splat_bin_shaped(gg_particles* ps, gg_volume* vol, const SplatUniforms* u, uint32_t edge, uint32_t chunk) {
     gg_context* ctx = vol->ctx;
     if (edge == 0u) {
-        SplatArgs a{ps->pos, ps->vel, vol->sums, *u, ps->first_index};
+        SplatArgs a{ps->pos, ps->vel, vol->sums, *u, ps->first_index, peer_sums(vol)};
         bin_kernel<<<(ps->count + 255u) / 256u, 256, 0, ctx->stream>>>(a);
         return gg::launch_status("splat bin");
     }
@@ -650,6 +686,7 @@ static int splat_bin_shaped(gg_particles* ps, gg_volume* vol, const SplatUniform
         vol->brick_counts_zero = true;
     }
     BrickArgs a;
+    a.peers = peer_sums(vol);
     a.pos = ps->pos;
     a.vel = ps->vel;
     a.sums = vol->sums;
@@ -781,6 +818,7 @@ GG_API void gg_volume_destroy(gg_volume* vol) {
     std::lock_guard<std::recursive_mutex> lock(ctx->mu);
     cudaSetDevice(ctx->device);
     cudaStreamSynchronize(ctx->stream);
+    close_peers(vol);
     if (vol->emission_tex) cudaDestroyTextureObject(vol->emission_tex);
     if (vol->velocity_tex) cudaDestroyTextureObject(vol->velocity_tex);
     if (vol->emission_surf) cudaDestroySurfaceObject(vol->emission_surf);
@@ -942,6 +980,42 @@ GG_API int gg_volume_sums(gg_volume* vol, void** device_words, uint64_t* words) 
         return gg::fail(GG_ERR_INVALID_ARGUMENT, "gg_volume_sums needs a volume and two outputs.");
     *device_words = vol->sums;
     *words = (uint64_t)vol->size * vol->size * vol->size * 6u;
+    return GG_OK;
+}
+
+GG_API int gg_volume_ipc_handle(gg_volume* vol, void* handle) {
+    if (!vol || !handle) return gg::fail(GG_ERR_INVALID_ARGUMENT, "gg_volume_ipc_handle needs a volume and an output.");
+    static_assert(sizeof(cudaIpcMemHandle_t) == GG_IPC_HANDLE_BYTES, "the handle size the header states");
+    std::lock_guard<std::recursive_mutex> lock(vol->ctx->mu);
+    GG_CUDA(cudaSetDevice(vol->ctx->device), "cudaSetDevice");
+    cudaIpcMemHandle_t h;
+    GG_CUDA(cudaIpcGetMemHandle(&h, vol->sums), "volume sums IPC handle");
+    std::memcpy(handle, &h, sizeof h);
+    return GG_OK;
+}
+
+GG_API int gg_volume_attach_peers(gg_volume* vol, const void* handles, uint32_t count) {
+    if (!vol || (count && !handles))
+        return gg::fail(GG_ERR_INVALID_ARGUMENT, "gg_volume_attach_peers needs a volume and the handles.");
+    if (count > GG_MAX_PEERS)
+        return gg::fail(GG_ERR_INVALID_ARGUMENT, "%u peers is more than the %d a volume attaches.", count,
+                        GG_MAX_PEERS);
+    std::lock_guard<std::recursive_mutex> lock(vol->ctx->mu);
+    GG_CUDA(cudaSetDevice(vol->ctx->device), "cudaSetDevice");
+    GG_CUDA(cudaStreamSynchronize(vol->ctx->stream), "peer detach");  // no deposit still adds into them
+    close_peers(vol);
+    for (uint32_t k = 0; k < count; ++k) {
+        cudaIpcMemHandle_t h;
+        std::memcpy(&h, static_cast<const char*>(handles) + (size_t)k * GG_IPC_HANDLE_BYTES, sizeof h);
+        void* p = nullptr;
+        const cudaError_t e = cudaIpcOpenMemHandle(&p, h, cudaIpcMemLazyEnablePeerAccess);
+        if (e != cudaSuccess) {
+            cudaGetLastError();
+            close_peers(vol);
+            return gg::fail(GG_ERR_DEVICE, "Peer %u's sums could not be opened (%s).", k, cudaGetErrorString(e));
+        }
+        vol->peer_sums[vol->peers++] = static_cast<uint32_t*>(p);
+    }
     return GG_OK;
 }
 

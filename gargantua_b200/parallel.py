@@ -18,6 +18,14 @@ On GPUs the all-reduce runs on the sums in device memory over NCCL, ordered
 on the context's stream between the bin and the resolve. Under the gloo
 backend (CPU process groups) the words pass through the host, widened to 64
 bits and folded back to 32, which is the same modular sum.
+
+With reduce="peer" there is no separate all-reduce: every rank opens the
+other ranks' sums through CUDA IPC (gg_volume_attach_peers), and the
+deposit adds each word into its own grid and into every peer's over NVLink
+(peer atomics), so when all ranks' bins are done every grid holds the total.
+The ranks only order themselves on the host: a barrier before the bin (no
+rank adds into a grid whose owner has not resolved and cleared the previous
+frame) and one after it (no rank resolves before every deposit has landed).
 """
 from __future__ import annotations
 
@@ -78,6 +86,29 @@ def sum_words_(words, group=None) -> None:
     dist.all_reduce(wide, op=dist.ReduceOp.SUM, group=group)
     wide &= 0xFFFFFFFF
     words.copy_(torch.where(wide >= 1 << 31, wide - (1 << 32), wide).to(torch.int32))
+
+
+def attach_peer_sums(vol: H.Volume, group=None) -> int:
+    """Exchange the volumes' IPC handles over the group and attach every
+    other rank's sums to `vol` (gg_volume_attach_peers); returns the number
+    attached. Every rank's volume must have the same size."""
+    import torch
+    import torch.distributed as dist
+
+    handle = (C.c_uint8 * T.IPC_HANDLE_BYTES)()
+    check(lib().gg_volume_ipc_handle(vol.handle, handle))
+    mine = torch.tensor(list(bytes(handle)) + [vol.size], dtype=torch.int64)
+    if _backend(group) == "nccl":
+        mine = mine.cuda(vol.ctx.device)
+    world, rank = dist.get_world_size(group), dist.get_rank(group)
+    everyone = [torch.zeros_like(mine) for _ in range(world)]
+    dist.all_gather(everyone, mine, group=group)
+    others = [t.cpu() for r, t in enumerate(everyone) if r != rank]
+    if any(int(t[-1]) != vol.size for t in others):
+        raise ValueError("every rank's volume must have the same size")
+    buf = bytes(b for t in others for b in t[:-1].to(torch.uint8).tolist())
+    check(lib().gg_volume_attach_peers(vol.handle, C.c_char_p(buf) if buf else None, len(others)))
+    return len(others)
 
 
 def host_records(em: np.ndarray, mo: np.ndarray, ma: np.ndarray) -> np.ndarray:
@@ -149,7 +180,9 @@ class ShardedDisk:
 
     def __init__(self, ctx: H.Context, count: int, size: int, seed: int = 1,
                  potential: int = T.POTENTIAL_PACZYNSKI_WIITA, group=None, rank: int | None = None,
-                 world: int | None = None):
+                 world: int | None = None, reduce: str = "collective"):
+        if reduce not in ("collective", "peer"):
+            raise ValueError(f"reduce is 'collective' or 'peer', not {reduce!r}")
         if rank is None or world is None:
             import torch.distributed as dist
 
@@ -163,6 +196,9 @@ class ShardedDisk:
         self.ctx = ctx
         self.particles = H.Particles(ctx, n, seed, potential, first_index=first)
         self.volume = H.Volume(ctx, size)
+        self.reduce = reduce
+        if reduce == "peer":
+            attach_peer_sums(self.volume, group)
 
     def advance(self, dispatches: int, seed_first: bool = False) -> None:
         self.particles.advance(dispatches, seed_first)
@@ -170,12 +206,33 @@ class ShardedDisk:
     def bin(self, exact: bool = True) -> None:
         self.volume.bin(self.particles, exact)
 
-    def splat(self, exact: bool = True) -> None:
+    def _barrier(self) -> None:
+        import torch.distributed as dist
+
+        self.ctx.synchronize()  # this rank's device work is done before it says so
+        dist.barrier(group=self.group)
+
+    def reduce_bin(self, exact: bool = True) -> None:
+        """Every rank's shard binned into every rank's sums (reduce="peer"):
+        after it, each rank's sums hold the unsharded grid."""
+        self._barrier()
         self.bin(exact)
-        combine_sums(self.volume, self.group)
+        self._barrier()
+
+    def splat(self, exact: bool = True) -> None:
+        if self.reduce == "peer":
+            self.reduce_bin(exact)
+        else:
+            self.bin(exact)
+            combine_sums(self.volume, self.group)
         self.volume.resolve()
         self.volume.frame += 1
 
     def close(self) -> None:
+        if self.reduce == "peer" and self.volume.handle:
+            # Unmap the other ranks' sums, and let every rank do so, before
+            # any rank frees the sums the others have mapped.
+            check(lib().gg_volume_attach_peers(self.volume.handle, None, 0))
+            self._barrier()
         self.volume.close()
         self.particles.close()

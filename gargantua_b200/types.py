@@ -161,6 +161,7 @@ SCHEDULE_CHUNKS, SCHEDULE_LANE_REFILL = 0, 1
 
 
 FP64_ESCAPING, FP64_ALL_FLAGGED = 0, 1
+IPC_HANDLE_BYTES, MAX_PEERS = 64, 7  # GG_IPC_HANDLE_BYTES, GG_MAX_PEERS
 SERVE_BATCHED, SERVE_SERIAL_PLAIN, SERVE_SERIAL_PLAIN_AS_WRITTEN = 0, 1, 2
 REQUEST_NO_STARS, REQUEST_NO_REDSHIFT, REQUEST_BAKE = 1, 2, 4
 

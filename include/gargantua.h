@@ -217,6 +217,23 @@ GG_API int gg_splat_autotune(gg_particles* ps, gg_volume* vol, const SplatUnifor
  * the volume is destroyed. */
 GG_API int gg_volume_sums(gg_volume* vol, void** device_words, uint64_t* words);
 
+/* The all-reduce done by the deposit itself, over peer memory. Each rank
+ * (one process per GPU) exports its volume's sums as a CUDA IPC handle
+ * (GG_IPC_HANDLE_BYTES bytes) and attaches the other ranks' handles, volumes
+ * of the same size; from then on gg_splat_bin adds every deposit word into
+ * its own sums and into each attached rank's, with peer atomics over
+ * NVLink, so once every rank's bin has finished each grid holds the sum of
+ * all shards, bit for bit as the integer all-reduce gives it, with no
+ * separate collective. The ranks order themselves on the host: every
+ * rank's previous resolve (which clears its sums) finishes before any rank
+ * bins, and every bin finishes before any rank resolves. At most
+ * GG_MAX_PEERS peers; count 0 detaches. No reference counterpart: the
+ * reference renders on one GPU. */
+#define GG_IPC_HANDLE_BYTES 64
+#define GG_MAX_PEERS 7
+GG_API int gg_volume_ipc_handle(gg_volume* vol, void* handle);
+GG_API int gg_volume_attach_peers(gg_volume* vol, const void* handles, uint32_t count);
+
 /* Copy the resolved textures to host arrays of n^3 half4 (IEEE binary16 bit
  * patterns, x fastest). Replaces Validate.readVolume (Validate.swift:204-230). */
 GG_API int gg_volume_read(gg_volume* vol, uint16_t* emission_half4, uint16_t* velocity_half4);

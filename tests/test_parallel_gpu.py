@@ -7,8 +7,13 @@ is then run under a one-rank NCCL group (device all-reduce on the context's
 stream) and a one-rank gloo group (through the host): both must give the
 volume one unsharded splat gives. More than one rank needs more GPUs than a
 test here has; the multi-rank logic runs on the CPU in test_parallel.py.
+The peer-memory reduce runs as two processes sharing the one GPU: each opens
+the other's sums through CUDA IPC and deposits into both, ordered by gloo
+barriers on the host (no kernel waits on another process's).
 """
+import os
 import socket
+import time
 
 import numpy as np
 import pytest
@@ -127,3 +132,74 @@ def test_sharded_disk_one_rank_matches_plain_splat(ctx, backend):
         whole.close()
     finally:
         dist.destroy_process_group()
+
+
+def _peer_rank(rank: int, world: int, port: int, outdir: str) -> None:
+    """One rank of the peer-memory reduce on GPU 0: its shard deposited into
+    every rank's sums (gg_volume_attach_peers), then two splats through
+    ShardedDisk.splat. Writes its sums and textures to outdir."""
+    import datetime
+
+    import torch.distributed as dist
+
+    import gargantua_b200 as g
+    from gargantua_b200 import parallel as P
+
+    dist.init_process_group("gloo", init_method=f"tcp://127.0.0.1:{port}", rank=rank, world_size=world,
+                            timeout=datetime.timedelta(seconds=120))
+    try:
+        ctx = g.Context(0)
+        disk = P.ShardedDisk(ctx, COUNT, SIZE, seed=SEED, reduce="peer")
+        disk.advance(40, seed_first=True)
+        disk.reduce_bin(exact=True)
+        em, mo, ma = disk.volume.read_sums()
+        np.savez(os.path.join(outdir, f"sums{rank}.npz"), em=em, mo=mo, ma=ma)
+        disk.volume.clear()
+        textures = []
+        for exact in (False, True):  # frames 0 and 1: the resolve clears, the barriers order the ranks
+            disk.splat(exact=exact)
+            textures.extend(disk.volume.read())
+        np.savez(os.path.join(outdir, f"tex{rank}.npz"), *textures)
+        disk.close()
+        ctx.close()
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
+def test_peer_memory_reduce_matches_the_unsharded_grid(ctx, tmp_path):
+    """reduce="peer": two ranks' deposits land in both grids over peer memory
+    (CUDA IPC), and each rank's sums and resolved volume equal one unsharded
+    splat's, exact and stochastic."""
+    import torch.multiprocessing as mp
+
+    import gargantua_b200 as g
+
+    procs = mp.start_processes(_peer_rank, args=(2, _port(), str(tmp_path)), nprocs=2, start_method="spawn",
+                               join=False)
+    deadline = time.time() + 300
+    while not procs.join(timeout=5):
+        if time.time() > deadline:
+            for p in procs.processes:
+                p.kill()
+            pytest.fail("the two ranks did not finish in 300 s")
+    whole = g.Particles(ctx, COUNT, SEED)
+    whole.advance(40, seed_first=True)
+    vol = g.Volume(ctx, SIZE)
+    vol.bin(whole, exact=True)
+    ref = vol.read_sums()
+    vol.clear()
+    ref_tex = []
+    for exact in (False, True):
+        vol.splat(whole, exact=exact)
+        ref_tex.extend(vol.read())
+    assert ref[2].any()
+    for rank in range(2):
+        got = np.load(tmp_path / f"sums{rank}.npz")
+        for name, r in zip(("em", "mo", "ma"), ref):
+            assert np.array_equal(got[name], r), (rank, name)
+        tex = np.load(tmp_path / f"tex{rank}.npz")
+        for k, r in enumerate(ref_tex):
+            assert np.array_equal(tex[f"arr_{k}"].view(np.uint16), r.view(np.uint16)), (rank, k)
+    vol.close()
+    whole.close()
