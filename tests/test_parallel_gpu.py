@@ -134,6 +134,33 @@ def test_sharded_disk_one_rank_matches_plain_splat(ctx, backend):
         dist.destroy_process_group()
 
 
+def test_peer_attach_refusals(ctx):
+    """gg_volume_attach_peers refuses more than GG_MAX_PEERS handles before
+    opening any, leaving the volume unattached (it still bins like a plain
+    volume); count 0 detaches nothing harmlessly; the volume exports a
+    handle."""
+    import ctypes as C
+
+    import gargantua_b200 as g
+    from gargantua_b200._lib import check
+
+    vol = g.Volume(ctx, 16)
+    lib = g.lib()
+    handles = bytes(64 * (g.types.MAX_PEERS + 1))
+    with pytest.raises(g.GargantuaError):
+        check(lib.gg_volume_attach_peers(vol.handle, C.c_char_p(handles), g.types.MAX_PEERS + 1))
+    check(lib.gg_volume_attach_peers(vol.handle, None, 0))
+    handle = (C.c_uint8 * g.types.IPC_HANDLE_BYTES)()
+    check(lib.gg_volume_ipc_handle(vol.handle, handle))
+    assert any(bytes(handle))
+    ps = g.Particles(ctx, 5000, SEED)
+    ps.advance(5, seed_first=True)
+    vol.bin(ps, exact=True)
+    assert vol.read_sums()[2].any()
+    ps.close()
+    vol.close()
+
+
 def _peer_rank(rank: int, world: int, port: int, outdir: str) -> None:
     """One rank of the peer-memory reduce on GPU 0: its shard deposited into
     every rank's sums (gg_volume_attach_peers), then two splats through
