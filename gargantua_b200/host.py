@@ -192,6 +192,7 @@ class Context:
         self.handle = C.c_void_p()
         self.device = device
         self._children = weakref.WeakSet()
+        self._pinned_cache: dict[int, list[int]] = {}  # released page-locked blocks by size (pinned_array)
         check(lib().gg_context_create(device, budget_bytes, C.byref(self.handle)))
 
     def adopt(self, child) -> None:
@@ -202,6 +203,10 @@ class Context:
         if self.handle:
             for child in list(self._children):
                 child.close()
+            for blocks in self._pinned_cache.values():
+                for address in blocks:
+                    lib().gg_host_free(address)
+            self._pinned_cache.clear()
             lib().gg_context_destroy(self.handle)
             self.handle = C.c_void_p()
 
@@ -616,20 +621,45 @@ class RequestSpec:
     volume: "Volume | None" = None  # None: the server's volume
 
 
+PINNED_CACHE_PER_SIZE = 4  # released blocks a context keeps for reuse, per size
+
+
 def pinned_array(ctx: Context, shape, dtype=np.float16) -> np.ndarray:
     """A numpy array in page-locked host memory (gg_host_alloc): the
-    library's copies into or out of it run at the link's rate. The memory is
-    released (gg_host_free) once the array and every view of it are gone."""
+    library's copies into or out of it run at the link's rate. Page-locking
+    costs time of its own, so once the array and every view of it are gone
+    the block goes back to the context, which hands it to the next array of
+    the same size (up to PINNED_CACHE_PER_SIZE kept per size) and releases
+    it (gg_host_free) when it closes. The contents start undefined."""
     dtype = np.dtype(dtype)
     shape = tuple(int(x) for x in (shape if isinstance(shape, (tuple, list)) else (shape,)))
     nbytes = int(np.prod(shape)) * dtype.itemsize
-    p = C.c_void_p()
-    check(lib().gg_host_alloc(ctx.handle, max(nbytes, 1), C.byref(p)))
+    size = max(nbytes, 1)
+    cached = ctx._pinned_cache.get(size)
+    if cached:
+        address = cached.pop()
+    else:
+        p = C.c_void_p()
+        check(lib().gg_host_alloc(ctx.handle, size, C.byref(p)))
+        address = p.value
+    owner = weakref.ref(ctx)
     free = lib().gg_host_free
-    address = p.value
-    # A ctypes array over the block whose finaliser frees it; numpy arrays
-    # made from it keep it alive through their base.
-    block_type = type("PinnedBlock", (C.c_char * max(nbytes, 1),), {"__del__": lambda self: free(address)})
+
+    def release(_block):
+        try:
+            c = owner()
+            if c is not None and c.handle:
+                kept = c._pinned_cache.setdefault(size, [])
+                if len(kept) < PINNED_CACHE_PER_SIZE:
+                    kept.append(address)
+                    return
+            free(address)
+        except Exception:
+            pass
+
+    # A ctypes array over the block whose finaliser hands it back; numpy
+    # arrays made from it keep it alive through their base.
+    block_type = type("PinnedBlock", (C.c_char * size,), {"__del__": release})
     block = block_type.from_address(address)
     return np.frombuffer(block, dtype=np.uint8, count=nbytes).view(dtype).reshape(shape)
 

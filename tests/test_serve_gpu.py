@@ -99,7 +99,8 @@ def test_each_result_is_the_same_alone_and_in_the_mix(world):
 def test_page_locked_outputs_match_pageable_ones(world):
     """gg_host_alloc / gg_host_free: a request served into page-locked memory
     (Server.submit's default) gives the pixels a pageable array gets, a view
-    outlives its array, and blocks are released as their arrays go."""
+    outlives its array, and blocks go back to the context for reuse as
+    their arrays go."""
     import gc
 
     import gargantua_b200 as g
@@ -116,11 +117,14 @@ def test_page_locked_outputs_match_pageable_ones(world):
     gc.collect()
     assert np.array_equal(copy.view(np.uint16), view.view(np.uint16))  # the view still reads the block
     server.close()
-    for _ in range(64):  # 64 MB allocated and released in turn
+    addresses = set()
+    for _ in range(64):  # one 1 MB block, handed back and reused
         block = g.pinned_array(world["ctx"], (1 << 20,), np.uint8)
         block[:] = 7
         assert int(block.sum()) == 7 << 20
+        addresses.add(block.__array_interface__["data"][0])
         del block
+    assert len(addresses) == 1
     import ctypes as C
 
     from gargantua_b200._lib import check
