@@ -173,20 +173,19 @@ def serve_slice(server, slice_, pinned):
     return results, wall, tot["span_seconds"], tot["busy_seconds"], tot["launches"]
 
 
-def pinned_outputs(slice_):
-    import torch
+def pinned_outputs(ctx, slice_):
+    """The slice's output arrays in page-locked host memory, from the
+    library's own allocator (gargantua_b200.pinned_array, gg_host_alloc), as
+    a host serving many requests would pass them."""
+    import gargantua_b200 as g
 
-    outs = []
-    for q in slice_:
-        t = torch.empty((q["width"] * q["height"], 4), dtype=torch.float16, pin_memory=torch.cuda.is_available())
-        outs.append(t.numpy())
-    return outs
+    return [g.pinned_array(ctx, (q["width"] * q["height"], 4), np.float16) for q in slice_]
 
 
 def latency_replay(server, stream):
     """Open loop: submit each request at its arrival time; latency is result
     ready minus arrival (gg_request_result.finished - submitted)."""
-    pinned = pinned_outputs(stream)
+    pinned = pinned_outputs(server.ctx, stream)
     t0 = time.perf_counter()
     base = stream[0]["t"]
     tickets = []
@@ -234,7 +233,7 @@ def class_table(servers: dict) -> list:
             for kerr in (False, True):
                 seed += 1
                 reqs = class_requests(w, h, cap, kerr, seed)
-                pins = pinned_outputs(reqs)
+                pins = pinned_outputs(next(iter(servers.values())).ctx, reqs)
                 row = {"class": f"{w}x{h}/{cap}/{'kerr' if kerr else 'schw'}", "requests": len(reqs)}
                 for name, server in servers.items():
                     serve_slice(server, reqs, pins)
@@ -636,9 +635,9 @@ def main():
             dist.barrier()
 
     for s in slices[:args.warmup]:
-        serve_slice(batched, s, pinned_outputs(s))
+        serve_slice(batched, s, pinned_outputs(ctx, s))
     timed = slices[args.warmup:]
-    pins = [pinned_outputs(s) for s in timed]
+    pins = [pinned_outputs(ctx, s) for s in timed]
     clocks = ClockSampler(local)
     barrier()
     clocks.start()
@@ -688,7 +687,7 @@ def main():
     # written, and this library's plain FP32 step arithmetic launched per
     # request (what batching and compensation add over it).
     def plain_baseline(server_plain):
-        serve_slice(server_plain, slices[0], pinned_outputs(slices[0]))
+        serve_slice(server_plain, slices[0], pinned_outputs(ctx, slices[0]))
         barrier()
         sampler = ClockSampler(local)
         sampler.start()
