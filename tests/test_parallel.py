@@ -94,6 +94,13 @@ def test_shard_bounds_partition_the_range():
         P.shard_bounds(10, 2, 2)
 
 
+def test_sharded_disk_refuses_an_unknown_reduce():
+    """reduce is "collective" (NCCL or the host) or "peer" (the deposit over
+    peer memory); anything else is refused before a particle is made."""
+    with pytest.raises(ValueError):
+        P.ShardedDisk(None, 10, 8, rank=0, world=1, reduce="ring")
+
+
 def test_rows_and_deal_cover_everything_once():
     rows = [P.rows_for_rank(1080, r, 8) for r in range(8)]
     assert rows[0][0] == 0 and rows[-1][1] == 1080
