@@ -226,7 +226,9 @@ GG_API int gg_volume_sums(gg_volume* vol, void** device_words, uint64_t* words);
  * all shards, bit for bit as the integer all-reduce gives it, with no
  * separate collective. The ranks order themselves on the host: every
  * rank's previous resolve (which clears its sums) finishes before any rank
- * bins, and every bin finishes before any rank resolves. At most
+ * bins, every bin finishes before any rank resolves, and every rank has
+ * detached (count 0, or destroyed its volume) before any rank destroys the
+ * volume the others have attached. At most
  * GG_MAX_PEERS peers; count 0 detaches. No reference counterpart: the
  * reference renders on one GPU. */
 #define GG_IPC_HANDLE_BYTES 64
