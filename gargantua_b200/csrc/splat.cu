@@ -367,8 +367,9 @@ template <uint32_t B> constexpr uint32_t deposit_min_blocks() { return B == 16u 
 //            and maximum, one shared atomic per warp);
 //   flush    the tile rows inside that range (a row is T cells along x, 6 T
 //            words, contiguous in the sums as well), one warp per row: each
-//            non-zero word is added to the sums with one global atomic and
-//            zeroed again in the tile, so the next item finds a zero tile.
+//            non-zero word is added to the sums (and to each attached
+//            peer's copy) with one global atomic and zeroed again in the
+//            tile, so the next item finds a zero tile.
 // Cells outside the range hold no deposit: a particle's corners lie at its
 // low corner or one voxel above it on each axis.
 template <uint32_t B>
